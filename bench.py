@@ -1,0 +1,473 @@
+#!/usr/bin/env python
+"""Benchmark: split-operator BM4 steps/s on H_2D 1024^2 (real time, length gauge, FP64).
+
+Workload (one "step" = one BM4 time step with its observables):
+  1024 x 1024 grid, DR = 0.2, dt = 0.05 a.u., V = -1/sqrt(x^2 + y^2 + 0.64); initial state
+  from imaginary time; 800 nm, 1e14 W/cm^2, 8-cycle sin^2 pulse (cos2 envelope), linear
+  polarisation along x, length gauge; cos^(1/8) absorbing mask over the outer 10% of each axis;
+  observables norm, dipole (x, y) and dipole acceleration (x, y) at every step. Synthetic inputs
+  only (no dataset).
+
+Reported (one JSON line on rank 0):
+  value      device-resident steps/s over all ranks (inputs already in HBM, the L2 flushed
+             with a 256 MB write between timed steps, CUDA events per step, max over ranks)
+  e2e        the same steps through the public C ABI with pinned host buffers: state upload,
+             qnd_run_length (field H2D and observable D2H every step), state download
+  roofline   the fused axis-pass kernel: algorithmic bytes per launch / its mean event time
+  cpu_baseline  the reference's own C code for this loop on the host cores (N=1, rank 0)
+  mixed      the same steps in mixed precision (complex64 bulk, FP64 reductions) and its
+             observable error against the FP64 run
+  cufft_yardstick  the same transform sequence with torch.fft (cuFFT), timed only
+
+--impl reference runs the reference's CPU implementation instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+NR, DR, DT, INTEG = 1024, 0.2, 0.05, "BM4"
+SOFT = 0.64
+OBS = ["norm", "dipole_r", "accel"]
+METRIC = "split-op steps/s (H_2D 1024^2, BM4, FP64, length gauge, obs every step)"
+FLUSH_BYTES = 256 << 20
+
+
+def workload_arrays():
+    from tdse_nd_mpi_b200.field import Mode, field_samples
+
+    x = -0.5 * DR * NR + np.arange(NR) * DR
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    r2 = X * X + Y * Y
+    V = -1.0 / np.sqrt(r2 + SOFT)
+    grads = [X / (r2 + SOFT) ** 1.5, Y / (r2 + SOFT) ** 1.5]
+    half = 0.5 * DR * NR
+    edge = 0.9 * half
+    ax = np.abs(x)
+    mask = np.ones(NR)
+    zone = ax > edge
+    mask[zone] = np.cos(0.5 * np.pi * (ax[zone] - edge) / (half - edge)).clip(0.0) ** 0.125
+    w = 45.5637639947958 / 800.0
+    tau = 8 * 2 * np.pi / w
+    E, A, t = field_samples(2, [Mode(1e14, 800.0, 0.0, 0.0, 0.0, tau, "cos2")], INTEG, DT, tau)
+    return V, grads, mask, E, t
+
+
+def gaussian_guess():
+    x = -0.5 * DR * NR + np.arange(NR) * DR
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    psi = np.exp(-(X * X + Y * Y) / 2.0).astype(np.complex128)
+    return psi / np.sqrt(np.sum(np.abs(psi) ** 2) * DR * DR)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.idx)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [p.strip() for p in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic():
+    p = os.path.join(ROOT, "profiles", "pass_kernel_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("bytes_per_launch"), d
+    return None, None
+
+
+# ------------------------------------------------------------------ CPU side --
+
+def cpu_reference_steps(max_steps, budget_s):
+    """Time the reference's own length-gauge loop (QuantumND_real.c:195-223) on this workload."""
+    from oracle import oracle as O
+
+    V, grads, mask, E, t = workload_arrays()
+    kind = "reference"
+    fast = False
+    try:
+        flags = open("/proc/cpuinfo").read()
+        fast = O.ref_available(fast=True) and (" avx2" in flags and " fma" in flags)
+    except OSError:
+        pass
+    nthreads = os.cpu_count() or 1
+    if O.ref_available(fast) or O.ref_available():
+        ctx = O.RefCtx(2, (NR, NR), (DR, DR), INTEG, DT, "H_2D", (0.0, 0.0), nthreads=nthreads, fast=fast)
+        ctx.set_vpot(V)
+        build = "reference sources, -O3 -ffast-math (its Makefile flags)" if fast else "reference sources, -O2 IEEE"
+        names = ["dipole_r"]
+    else:
+        kind = "port"
+        ctx = O.OracleCtx(2, (NR, NR), (DR, DR), INTEG, DT, nthreads=nthreads)
+        ctx.set_vpot(V)
+        for j in range(2):
+            ctx.set_gradv(j, grads[j])
+            ctx.set_mask_axis(j, mask)
+        build = "C restatement (oracle/qnd_oracle.c)"
+        names = ["norm", "dipole_r", "accel"]
+    psi = gaussian_guess()
+    i0 = len(t) // 2
+    # one call of k steps costs 2 representation changes + k loop bodies: time a 1-step call and a
+    # k-step call and take the difference, so the per-step figure is exactly the loop body's.
+    t_a = time.perf_counter()
+    ctx.run_length(psi, E[i0:i0 + 1], names)
+    t1 = time.perf_counter() - t_a
+    k = int(max(3, min(max_steps, budget_s / max(t1, 1e-6))))
+    t_a = time.perf_counter()
+    ctx.run_length(psi, E[i0 + 1:i0 + 1 + k], names)
+    tk = time.perf_counter() - t_a
+    per_step = (tk - t1) / (k - 1)
+    sample = (f"{k} + 1 BM4 length-gauge steps of the H_2D 1024^2 workload with per-step {'+'.join(names)} "
+              f"(loop of QuantumND_real.c:195-223), {build}, FFTW-API shim FFT (radix-2, OpenMP over lines), "
+              f"{nthreads} threads; per-step time = (t[{k} steps] - t[1 step]) / {k - 1}")
+    return {"value": 1.0 / per_step, "unit": "steps/s", "cores": nthreads, "kind": kind, "sample": sample}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    budget = float(os.environ.get("QND_REF_BUDGET_S", "150"))
+    res = cpu_reference_steps(args.steps, budget)
+    line = {
+        "metric": METRIC, "value": res["value"], "unit": "steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 / res["value"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": "H_2D 1024x1024 real-time BM4 length gauge, dt=0.05, obs every step", "nr": [NR, NR],
+                   "dr": DR, "dt": DT, "integrator": INTEG, "parallelism": "replicas only",
+                   "l2": "state 16.8 MB; CPU run"},
+        "cpu_baseline": res,
+        "e2e": {"value": res["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU side --
+
+def cufft_yardstick(torch, V, E, steps):
+    """The same per-step transform sequence (14 full 2-D transforms) with torch.fft (cuFFT)."""
+    dev = torch.device("cuda")
+    from tdse_nd_mpi_b200.field import integrator_coeffs
+
+    asc = integrator_coeffs(INTEG, DT)
+    s = len(asc) // 2
+    p = 2 * np.pi * np.fft.fftfreq(NR, d=DR)
+    KX, KY = np.meshgrid(p, p, indexing="ij")
+    kin = torch.tensor(0.5 * (KX ** 2 + KY ** 2), device=dev)
+    x = -0.5 * DR * NR + np.arange(NR) * DR
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    Xt, Yt = torch.tensor(X, device=dev), torch.tensor(Y, device=dev)
+    Vt = torch.tensor(V, device=dev)
+    psi = torch.tensor(gaussian_guess(), device=dev)
+    kc = [asc[0]] + [asc[2 * i - 1] + asc[2 * i] for i in range(1, s)] + [asc[2 * s - 1]]
+    kph = [torch.exp(-1j * c * kin) for c in kc]
+    hs = [asc[2 * i] + asc[2 * i + 1] for i in range(s)]
+
+    def step(k):
+        nonlocal psi
+        ph = torch.fft.fft2(psi)
+        for i in range(s):
+            psi_r = torch.fft.ifft2(kph[i] * ph)
+            ex, ey = float(E[k, i, 0]), float(E[k, i, 1])
+            psi_r = psi_r * torch.exp(-1j * hs[i] * (Vt + Xt * ex + Yt * ey))
+            ph = torch.fft.fft2(psi_r)
+        psi = torch.fft.ifft2(kph[s] * ph)
+        return (psi.abs() ** 2).sum()
+
+    for k in range(3):
+        step(k)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for k in range(steps):
+        step(k)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    return {"value": 1000.0 / ms, "unit": "steps/s", "ms_per_step": ms,
+            "what": "torch.fft fft2/ifft2 (cuFFT) with torch elementwise phases: 14 transforms per BM4 step, "
+                    "no mask, reduction only of the norm; timed only, not on any product path"}
+
+
+def setup_grid(torch, precision, V, grads, mask, stream):
+    from tdse_nd_mpi_b200 import Grid
+
+    g = Grid(2, (NR, NR), (DR, DR), INTEG, DT, precision=precision)
+    g.set_stream(stream.cuda_stream)
+    g.set_potential(V)
+    for j in range(2):
+        g.set_gradv(j, grads[j])
+        g.set_mask_axis(j, mask)
+    return g
+
+
+def ground_state(torch, V, stream):
+    """Initial state: 100 imaginary-time BM4 steps (dt = 0.05) from a Gaussian, on the GPU."""
+    from tdse_nd_mpi_b200 import Grid
+
+    gi = Grid(2, (NR, NR), (DR, DR), INTEG, DT)
+    gi.set_stream(stream.cuda_stream)
+    gi.set_potential(V)
+    st = gi.state(gaussian_guess())
+    gi.imag_propagate([st], 0, 100)
+    psi = st.download()
+    st.free()
+    gi.close()
+    return psi
+
+
+def timed_steps(torch, grid, psi_t, E_dev, obs_dev, names, i0, steps, warmup, flush):
+    """Warm-up, then `steps` single-step calls each bracketed by CUDA events, the L2 flushed between."""
+    for k in range(warmup):
+        flush.zero_()
+        grid.run_length_dev(psi_t, E_dev[i0 + k], 1, names, obs_dev[k])
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for k in range(steps):
+        flush.zero_()
+        starts[k].record()
+        grid.run_length_dev(psi_t, E_dev[i0 + warmup + k], 1, names, obs_dev[warmup + k])
+        ends[k].record()
+    torch.cuda.synchronize()
+    return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-extras", action="store_true", help="skip mixed / cuFFT / CPU legs")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+
+    V, grads, mask, E, t = workload_arrays()
+    nsteps_avail = E.shape[0]
+    i0 = nsteps_avail // 2 - (args.steps + args.warmup) // 2
+    i0 = max(0, min(i0, nsteps_avail - args.steps - args.warmup))
+    psi0 = ground_state(torch, V, stream)
+    grid = setup_grid(torch, "fp64", V, grads, mask, stream)
+    nv = grid.nvalues(OBS)
+    dev = torch.device("cuda", local)
+    E_dev = torch.tensor(E, device=dev).contiguous()
+    obs_dev = torch.zeros((args.steps + args.warmup, nv), dtype=torch.float64, device=dev)
+    psi_t = torch.tensor(psi0.view(np.float64), device=dev).contiguous()   # complex128 as interleaved doubles
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    # ---- timed region (value)
+    grid.get_profile(reset=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        total_ms = timed_steps(torch, grid, psi_t, E_dev, obs_dev, OBS, i0, args.steps, args.warmup, flush)
+    launches, _, _ = grid.get_profile(reset=True)
+    per_step_launches = launches / (args.steps + args.warmup)
+    gpu_launches = int(round(per_step_launches * args.steps))
+    if dist:
+        tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    value = world * args.steps / (total_ms / 1000.0)
+    ms_step = total_ms / args.steps
+    obs_fp64 = obs_dev[args.warmup:].cpu().numpy()
+
+    # ---- roofline of the fused pass kernel (per-launch CUDA events, L2 flushed between steps)
+    grid.set_profiling(True)
+    prof_steps = min(args.steps, 100)
+    psi_t2 = torch.tensor(psi0.view(np.float64), device=dev).contiguous()
+    timed_steps(torch, grid, psi_t2, E_dev, obs_dev, OBS, i0, prof_steps, 0, flush)
+    _, passes, pass_ms = grid.get_profile(reset=True)
+    grid.set_profiling(False)
+    n = NR * NR
+    bytes_per_pass = 2 * n * 16
+    passes_per_step = passes / prof_steps
+    avg_pass_s = pass_ms / passes / 1000.0
+    peak, peak_src = measured_peak()
+    achieved = bytes_per_pass / avg_pass_s / 1e9
+    traffic, _ = committed_traffic()
+    step_bytes = passes_per_step * bytes_per_pass
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)" if peak_src == "measured"
+                else "fallback 6650 GB/s",
+                "kernel": "qnd_pass_kernel<double,1024> (fused FFT/phase/iFFT axis pass)",
+                "bytes_per_launch": bytes_per_pass, "mean_launch_us": avg_pass_s * 1e6,
+                "launches_per_step": passes_per_step,
+                "step_bytes": step_bytes, "step_frac_of_peak": (step_bytes / (ms_step / 1000.0) / 1e9) / peak}
+
+    # ---- e2e through the C ABI with pinned host buffers
+    import ctypes as C
+
+    from tdse_nd_mpi_b200 import _lib
+
+    e2e_steps = args.steps
+    E_host = torch.tensor(E[i0:i0 + e2e_steps]).contiguous().pin_memory()
+    obs_host = torch.zeros((e2e_steps, nv), dtype=torch.float64).pin_memory()
+    psi_host = torch.tensor(psi0.view(np.float64)).contiguous().pin_memory()
+    psi_dev_e2e = torch.empty_like(psi_t)
+    names_c = (C.c_char_p * len(OBS))(*[s.encode() for s in OBS])
+    L = _lib.lib()
+    dptr = lambda tns: C.cast(C.c_void_p(tns.data_ptr()), C.POINTER(C.c_double))  # noqa: E731
+    flush.zero_()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    _lib.check(L.qnd_state_upload(grid.h, C.c_void_p(psi_dev_e2e.data_ptr()), dptr(psi_host)))
+    _lib.check(L.qnd_run_length(grid.h, C.c_void_p(psi_dev_e2e.data_ptr()), dptr(E_host), e2e_steps, len(OBS),
+                                names_c, dptr(obs_host)))
+    _lib.check(L.qnd_state_download(grid.h, dptr(psi_host), C.c_void_p(psi_dev_e2e.data_ptr())))
+    b.record()
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b)
+    if dist:
+        tt = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e = {"value": world * e2e_steps / (e2e_ms / 1000.0), "unit": "steps/s",
+           "h2d_bytes_per_step": (n * 16 + e2e_steps * grid.s * 2 * 8) / e2e_steps,
+           "d2h_bytes_per_step": (n * 16 + e2e_steps * nv * 8) / e2e_steps,
+           "what": "qnd_state_upload + qnd_run_length (host E, host observable rows) + qnd_state_download"}
+
+    extras = {}
+    if not args.no_extras:
+        # ---- mixed precision on the same steps, error vs the FP64 run
+        gm = setup_grid(torch, "mixed", V, grads, mask, stream)
+        psi_m = torch.tensor(psi0.astype(np.complex64).view(np.float32), device=dev).contiguous()
+        obs_m = torch.zeros_like(obs_dev)
+        ms_m = timed_steps(torch, gm, psi_m, E_dev, obs_m, OBS, i0, args.steps, args.warmup, flush) / args.steps
+        om = obs_m[args.warmup:].cpu().numpy()
+        scale = np.maximum(np.abs(obs_fp64), 1e-3 * np.max(np.abs(obs_fp64), axis=0))
+        rel_err = float(np.max(np.abs(om - obs_fp64) / scale))
+        extras["mixed"] = {"value": world * 1000.0 / ms_m, "ms_per_step": ms_m, "speedup_vs_fp64": ms_step / ms_m,
+                           "max_rel_obs_err_vs_fp64": rel_err, "dtype": "f32 bulk, f64 reductions"}
+        gm.close()
+        if rank == 0:
+            try:
+                extras["cufft_yardstick"] = cufft_yardstick(torch, V, E[i0:], min(args.steps, 50))
+            except Exception as exc:  # yardstick only
+                extras["cufft_yardstick"] = {"error": str(exc)}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        try:
+            cpu = cpu_reference_steps(40, float(os.environ.get("QND_CPU_BUDGET_S", "20")))
+        except Exception as exc:
+            cpu = {"value": None, "unit": "steps/s", "cores": os.cpu_count(), "kind": "unavailable",
+                   "sample": f"CPU baseline failed: {exc}"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "H_2D 1024x1024 real-time BM4 length gauge, dt=0.05, 800nm 1e14 W/cm^2 8-cycle "
+                               "sin^2, cos^(1/8) mask, norm+dipole+accel every step",
+                   "nr": [NR, NR], "dr": DR, "dt": DT, "integrator": INTEG, "parallelism": f"replicas x{world}",
+                   "l2": "state 16.8 MB < L2; 256 MB L2 flush between timed steps"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
+        "clocks": clk.summary(),
+    }
+    line.update(extras)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    grid.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,136 @@
+/*
+ * qnd.h — C ABI of the B200-native split-operator TDSE engine (libqnd_b200.so).
+ *
+ * This is the drop-in boundary for QuantumND's hot path (jonathan-dubois/
+ * TDSE_ND_MPI). It replaces, inside the reference's C drivers, the FFTW-MPI plans
+ * and every loop of integrators.c / calculate_observables.c / the Gram-Schmidt of
+ * QuantumND_imag.c. The whole N-D grid lives in one GPU's HBM.
+ *
+ * Conventions
+ *  - Every function returns QND_OK (0) or a non-zero QND_E* code; the message is
+ *    in qnd_last_error() (per host thread). The reference aborts instead
+ *    (MPI_Abort everywhere); drivers map non-zero codes to stderr + exit(1).
+ *  - Arrays are row-major with axis 0 slowest (meshgrid.c:205-211).
+ *  - Wavefunctions on the device ("psi_dev") are complex128 (interleaved re, im)
+ *    for QND_FP64 contexts and complex64 for QND_MIXED contexts; qnd_state_bytes()
+ *    gives the size. Host-side wavefunctions passed to qnd_state_upload/download are
+ *    always complex128 (C99 double complex), like the reference's arrays.
+ *  - Field samples E/A are host arrays laid out [nsteps][s][dim] exactly like
+ *    F.E / F.A (integrators.c:81-101).
+ *  - A context is bound to one CUDA device and one stream; it is not re-entrant.
+ *  - Observable names are the reference's (calculate_observables.c:48-56): "dipole_r",
+ *    "dipole_v", "energy", "Lz", and the zero-width "PMD", "PED", "wavefunction",
+ *    "none"; plus two extensions: "norm" (1 value) and "accel" (dim values,
+ *    -<dV/dx_j>, needs qnd_set_gradv).
+ */
+#ifndef QND_H
+#define QND_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QND_OK 0
+#define QND_EINVAL 1       /* bad argument */
+#define QND_ECUDA 2        /* CUDA runtime error */
+#define QND_ENOMEM 3       /* device allocation failed */
+#define QND_ENORM 4        /* Gram-Schmidt norm below 1e-12 (QuantumND_imag.c:297-304) */
+#define QND_EUNSUPPORTED 5 /* configuration outside what this build implements */
+
+#define QND_FP64 0  /* complex128 state, FP64 everywhere */
+#define QND_MIXED 1 /* complex64 state, FFT and phases in FP32, all reductions in FP64 */
+
+typedef struct qnd_ctx qnd_ctx;
+
+const char *qnd_version(void);
+const char *qnd_last_error(void);
+
+/* ---- context: replaces Initialize_meshgrid (meshgrid.c:17-179) and
+ *      Initialize_integrator (integrators.c:13-71). nr[j] must be a power of two
+ *      (parameters.c:72-76) between 2 and 4096. integrator: Verlet, BM4, BM6, RKN4. */
+int qnd_ctx_create(int dim, const int64_t *nr, const double *dr, const char *integrator, double dt, int precision,
+                   qnd_ctx **out);
+int qnd_ctx_destroy(qnd_ctx *ctx);
+/* Use an existing cudaStream_t (passed as void*); NULL selects the context's own stream. */
+int qnd_ctx_set_stream(qnd_ctx *ctx, void *stream);
+/* Grid facts: total points, stages s, as_scaled[0..2s) (integrators.c:64), dNr, dNp (meshgrid.c:23-28). */
+int qnd_ctx_info(qnd_ctx *ctx, int64_t *n_total, int *s_integrator, double *as_scaled, double *dNr, double *dNp);
+int qnd_state_bytes(qnd_ctx *ctx, int64_t *bytes_per_state);
+
+/* ---- potentials (meshgrid.c:133-153) */
+int qnd_set_potential_named(qnd_ctx *ctx, const char *name); /* H_1D H_2D H_3D Ne_2D Ne_short_2D Ar_2D Kr_2D Xe_2D */
+int qnd_set_potential(qnd_ctx *ctx, const double *vpot_host); /* custom V on the grid [N] */
+int qnd_set_cap(qnd_ctx *ctx, double strength, double length); /* quadratic CAP, meshgrid.c:133-135 */
+int qnd_set_vcap(qnd_ctx *ctx, const double *vcap_host);       /* custom CAP on the grid [N] */
+/* Extensions (no reference counterpart): dV/dx_axis on the grid for "accel"; a per-axis
+ * multiplicative mask m_axis[N_axis] applied to psi after every real-time step (NULL clears). */
+int qnd_set_gradv(qnd_ctx *ctx, int axis, const double *gradv_host);
+int qnd_set_mask_axis(qnd_ctx *ctx, int axis, const double *mask_host);
+
+/* ---- device state helpers (the reference allocates with fftw_alloc_complex,
+ *      QuantumND_imag.c:130, QuantumND_real.c:135) */
+int qnd_state_alloc(qnd_ctx *ctx, int64_t nstates, void **psi_dev);
+int qnd_state_free(qnd_ctx *ctx, void *psi_dev);
+int qnd_state_upload(qnd_ctx *ctx, void *psi_dev, const double *psi_host_c128);
+int qnd_state_download(qnd_ctx *ctx, double *psi_host_c128, const void *psi_dev);
+int qnd_synchronize(qnd_ctx *ctx);
+
+/* ---- split-operator steps (integrators.c:135-232), nsteps consecutive steps on the device */
+/* Integration_step_imag (integrators.c:135-163): psi in r-space. */
+int qnd_step_imag(qnd_ctx *ctx, void *psi_dev, int64_t nsteps);
+/* Integration_step_length (integrators.c:170-194): psi in the unitary p-representation
+ * (QuantumND_real.c:190-192); E host [nsteps][s][dim]. */
+int qnd_step_length(qnd_ctx *ctx, void *psi_p_dev, const double *E_host, int64_t nsteps);
+/* Integration_step_velocity (integrators.c:201-232): psi in r-space; A host [nsteps][s][dim]. */
+int qnd_step_velocity(qnd_ctx *ctx, void *psi_dev, const double *A_host, int64_t nsteps);
+/* Unitary representation changes used by the length-gauge driver (QuantumND_real.c:190-192, 200-202). */
+int qnd_to_p(qnd_ctx *ctx, void *psi_dev);
+int qnd_to_r(qnd_ctx *ctx, void *psi_dev);
+
+/* ---- driver loops */
+/* Real-time length gauge as QuantumND_real.c:188-229: psi_r_dev in r-space in and out;
+ * obs_host [nsteps][nvalues] receives the observables of psi(t_it) before step it, exactly the
+ * rows the reference writes (QuantumND_real.c:197-207). obs_host may be NULL when nobs == 0. */
+int qnd_run_length(qnd_ctx *ctx, void *psi_r_dev, const double *E_host, int64_t nsteps, int nobs,
+                   const char *const *names, double *obs_host);
+/* Real-time velocity gauge as QuantumND_real.c:168-187; alpha_host [nsteps][dim] = A(t_it) for
+ * the observables (the Field_vectors call at QuantumND_real.c:173). */
+int qnd_run_velocity(qnd_ctx *ctx, void *psi_r_dev, const double *A_host, const double *alpha_host, int64_t nsteps,
+                     int nobs, const char *const *names, double *obs_host);
+/* Gram_Schmidt_orthonormalization (QuantumND_imag.c:265-311) of states_dev[j] against
+ * states_dev[0..j); norm2_out (may be NULL) receives ||v||^2 dNr. QND_ENORM below 1e-12. */
+int qnd_gram_schmidt(qnd_ctx *ctx, void *const *states_dev, int j, double *norm2_out);
+/* The imaginary-time loop body of QuantumND_imag.c:182-185: nsteps x {step, Gram-Schmidt}. */
+int qnd_imag_propagate(qnd_ctx *ctx, void *const *states_dev, int j, int64_t nsteps);
+
+/* Device-resident variant of qnd_run_length for pipelines that keep the field and the
+ * observable rows on the GPU (no host synchronisation, no host copies): E_dev
+ * [nsteps][s][dim] and obs_dev [nsteps][nvalues] are device pointers, and row i holds the
+ * observables of psi after step i (the reference's row i+1). Same per-step work as the
+ * loop of QuantumND_real.c:195-223. */
+int qnd_run_length_dev(qnd_ctx *ctx, void *psi_r_dev, const double *E_dev, int64_t nsteps, int nobs,
+                       const char *const *names, double *obs_dev);
+
+/* ---- launch accounting (no reference counterpart; the reference only prints wall
+ *      times, QuantumND_real.c:231-235). When enabled, every fused-pass launch is
+ *      bracketed by CUDA events on the context's stream. */
+int qnd_ctx_set_profiling(qnd_ctx *ctx, int enable);
+/* Kernels launched since the last reset, pass launches timed, and their summed device time.
+ * Synchronises the stream. reset != 0 clears the counters afterwards. */
+int qnd_ctx_get_profile(qnd_ctx *ctx, int64_t *kernels_launched, int64_t *passes_timed, double *pass_ms_total,
+                        int reset);
+
+/* ---- observables (calculate_observables.c:89-266) */
+int qnd_observable_count(qnd_ctx *ctx, int nobs, const char *const *names, int *nvalues);
+/* Calculation_global_observables (calculate_observables.c:119-140) on an r-space psi; alpha [dim]. */
+int qnd_observables(qnd_ctx *ctx, const void *psi_r_dev, int nobs, const char *const *names, const double *alpha,
+                    double *out_host);
+/* Calculation_global_energies (calculate_observables.c:89-116): out[m] = Re <psi|H^(m+1)|psi> dNr. */
+int qnd_energies(qnd_ctx *ctx, const void *psi_r_dev, int n, double *out_host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QND_H */

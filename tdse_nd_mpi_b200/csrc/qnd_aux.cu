@@ -1,0 +1,148 @@
+// qnd_aux.cu — small kernels around the passes: Gram-Schmidt projections
+// (QuantumND_imag.c:265-311), r-space reductions, scaling, per-step field tables.
+#include "qnd_kernels.cuh"
+
+namespace qnd {
+
+// ---- Gram-Schmidt ---------------------------------------------------------------
+
+// c_k = sum conj(states[k]) * psi  for k in [k0, k0+nk): accumulators (re, im) pairs.
+template <typename R> __global__ void __launch_bounds__(256) gs_dot_kernel(const __grid_constant__ GSArgs<R> a) {
+    using V = cplx_t<R>;
+    double acc[MAX_RED];
+#pragma unroll
+    for (int k = 0; k < MAX_RED; ++k) acc[k] = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (long long)gridDim.x * blockDim.x) {
+        const V v = a.psi[i];
+#pragma unroll
+        for (int q = 0; q < MAX_RED / 2; ++q) {
+            if (q >= a.nk) break;
+            const V p = a.states[a.k0 + q][i];
+            acc[2 * q] += double(p.x) * double(v.x) + double(p.y) * double(v.y);
+            acc[2 * q + 1] += double(p.x) * double(v.y) - double(p.y) * double(v.x);
+        }
+    }
+    finish_red<256>(a.red, acc);
+}
+
+// psi <- psi - sum_k c_k states[k]; accumulate |psi|^2.
+template <typename R> __global__ void __launch_bounds__(256) gs_axpy_kernel(const __grid_constant__ GSArgs<R> a) {
+    using V = cplx_t<R>;
+    double acc[MAX_RED];
+#pragma unroll
+    for (int k = 0; k < MAX_RED; ++k) acc[k] = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (long long)gridDim.x * blockDim.x) {
+        V v = a.psi[i];
+        for (int k = 0; k < a.j; ++k) {
+            const V p = a.states[k][i];
+            const R cr = R(a.coef[2 * k]), ci = R(a.coef[2 * k + 1]);
+            v.x -= cr * p.x - ci * p.y;
+            v.y -= cr * p.y + ci * p.x;
+        }
+        a.psi[i] = v;
+        acc[0] += double(v.x) * double(v.x) + double(v.y) * double(v.y);
+    }
+    finish_red<256>(a.red, acc);
+}
+
+__global__ void gs_finalize_kernel(const double* norm2, double tol, double* scale, int* flag) {
+    const double n2 = *norm2;
+    if (n2 < tol || !(n2 == n2)) {
+        *flag = 1;
+        *scale = 1.0;
+    } else {
+        *scale = 1.0 / sqrt(n2);
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) scale_kernel(cplx_t<R>* psi, long long n, const double* scale_dev) {
+    const R s = R(*scale_dev);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        cplx_t<R> v = psi[i];
+        psi[i] = cplx_t<R>{v.x * s, v.y * s};
+    }
+}
+
+template <typename R> void launch_gs_dot(const GSArgs<R>& a, cudaStream_t st, int nblocks) {
+    gs_dot_kernel<R><<<nblocks, 256, 0, st>>>(a);
+}
+template <typename R> void launch_gs_axpy(const GSArgs<R>& a, cudaStream_t st, int nblocks) {
+    gs_axpy_kernel<R><<<nblocks, 256, 0, st>>>(a);
+}
+template <typename R> void launch_grid_reduce(const PassArgs<R>& a, long long n, cudaStream_t st, int nblocks) {
+    qnd_grid_reduce_kernel<R><<<nblocks, 256, 0, st>>>(a, n);
+}
+template <typename R> void launch_scale(cplx_t<R>* psi, long long n, const double* scale_dev, cudaStream_t st) {
+    long long nb = (n + 255) / 256;
+    if (nb > 148 * 8) nb = 148 * 8;
+    scale_kernel<R><<<(int)nb, 256, 0, st>>>(psi, n, scale_dev);
+}
+void launch_gs_finalize(const double* norm2, double tol, double* scale, int* flag, cudaStream_t st) {
+    gs_finalize_kernel<<<1, 1, 0, st>>>(norm2, tol, scale, flag);
+}
+
+// ---- per-step field tables ------------------------------------------------------
+
+template <typename R>
+__global__ void __launch_bounds__(256) field_tables_kernel(const __grid_constant__ FieldTableArgs a, cplx_t<R>* out) {
+    const long long total = (long long)a.nsteps * a.s * a.ntot;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const long long blk = i / a.ntot;
+        const int pos = int(i - blk * a.ntot);
+        const int ia = int(blk % a.s);
+        int ax = 0;
+        while (ax + 1 < a.dim && pos >= a.off[ax + 1]) ++ax;
+        const double f = a.field[blk * a.dim + ax];
+        const double x = a.axes[pos];
+        const double h = a.h[ia];
+        double theta, mag;
+        if (a.velocity) {
+            theta = h * (.5 * x * x + (x + .5 * f) * f);
+            mag = 1.0 / double(a.nr[ax]);
+        } else {
+            theta = h * (x * f);
+            mag = 1.0;
+        }
+        double sn, cs;
+        sincos(theta, &sn, &cs);
+        out[i] = cplx_t<R>{R(mag * cs), R(-mag * sn)};
+    }
+}
+
+template <typename R> void launch_field_tables(const FieldTableArgs& a, cplx_t<R>* out, cudaStream_t st) {
+    const long long total = (long long)a.nsteps * a.s * a.ntot;
+    long long nb = (total + 255) / 256;
+    if (nb > 148 * 16) nb = 148 * 16;
+    if (nb < 1) nb = 1;
+    field_tables_kernel<R><<<(int)nb, 256, 0, st>>>(a, out);
+}
+
+template <typename R>
+__global__ void axis_table_kernel(int mode, const double* p, int N, double alpha, void* out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < N; k += gridDim.x * blockDim.x) {
+        const double w = p[k] + alpha;
+        if (mode == 0) {
+            static_cast<double*>(out)[k] = w;
+        } else {
+            static_cast<cplx_t<R>*>(out)[k] = cplx_t<R>{R(w / double(N)), R(0)};
+        }
+    }
+}
+
+template <typename R> void launch_axis_table(int mode, const double* p, int N, double alpha, void* out, cudaStream_t st) {
+    axis_table_kernel<R><<<(N + 255) / 256, 256, 0, st>>>(mode, p, N, alpha, out);
+}
+
+#define QND_INST(R)                                                                               \
+    template void launch_gs_dot<R>(const GSArgs<R>&, cudaStream_t, int);                          \
+    template void launch_gs_axpy<R>(const GSArgs<R>&, cudaStream_t, int);                         \
+    template void launch_grid_reduce<R>(const PassArgs<R>&, long long, cudaStream_t, int);        \
+    template void launch_scale<R>(cplx_t<R>*, long long, const double*, cudaStream_t);            \
+    template void launch_field_tables<R>(const FieldTableArgs&, cplx_t<R>*, cudaStream_t);        \
+    template void launch_axis_table<R>(int, const double*, int, double, void*, cudaStream_t);
+QND_INST(double)
+QND_INST(float)
+#undef QND_INST
+
+}  // namespace qnd

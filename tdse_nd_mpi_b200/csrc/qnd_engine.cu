@@ -1,0 +1,1532 @@
+// qnd_engine.cu — host side of libqnd_b200.so: context, tables, pass schedules and
+// the extern "C" API declared in include/qnd.h.
+//
+// Representation: the engine keeps every state in r-space. A split-operator
+// sub-step of the reference, e.g. for the length gauge (integrators.c:170-194)
+//     psi_p <- K(b) F [ V(h) B K(a) psi_p ] / N
+// is, with chi = B psi_p / sqrt(N), the r-space product
+//     chi <- S(b) V(h) S(a) chi,   S(c) = B K(c) F / N.
+// The kinetic factor is separable (K = sum_j p_j^2/2), so S(c) = prod_j S_j(c): one
+// "sandwich" pass per axis (FFT along j, multiply by exp(-i c p_j^2/2)/N_j, inverse
+// FFT along j). Consecutive S(b) S(a') merge into S(b + a'), and V(h) -- the only
+// non-separable factor -- is applied in the epilogue of the last pass of each
+// sandwich. One sub-step therefore costs one read and one write of the state per
+// axis, and the observables at step boundaries (QuantumND_real.c:197-212) come out
+// of the last pass's fused reductions without the reference's extra transforms.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/qnd.h"
+#include "qnd_kernels.cuh"
+
+namespace qnd {
+
+static thread_local std::string g_err;
+
+struct Error {
+    int code;
+    std::string msg;
+};
+
+static std::string fmt(const char* f, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, f);
+    vsnprintf(buf, sizeof buf, f, ap);
+    va_end(ap);
+    return buf;
+}
+
+#define QND_FAIL(code, ...) throw ::qnd::Error{code, ::qnd::fmt(__VA_ARGS__)}
+#define QND_CK(x)                                                                                   \
+    do {                                                                                            \
+        cudaError_t e_ = (x);                                                                       \
+        if (e_ != cudaSuccess) QND_FAIL(QND_ECUDA, "%s: %s", #x, cudaGetErrorString(e_));           \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    void reset() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    void ensure(size_t b) {
+        if (b <= bytes && p) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, b ? b : 16);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            QND_FAIL(QND_ENOMEM, "cudaMalloc(%zu bytes): %s", b, cudaGetErrorString(e));
+        }
+        bytes = b;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+static PassKernelInfo lookup_pass(bool fp64, int L, bool strided, int mode) {
+#define QND_CASE(LL)                                                                                              \
+    case LL:                                                                                                      \
+        return fp64 ? pass_kernel_info<double, LL>(strided, mode) : pass_kernel_info<float, LL>(strided, mode);
+    switch (L) {
+        QND_CASE(2) QND_CASE(4) QND_CASE(8) QND_CASE(16) QND_CASE(32) QND_CASE(64) QND_CASE(128) QND_CASE(256)
+        QND_CASE(512) QND_CASE(1024) QND_CASE(2048) QND_CASE(4096)
+    default: QND_FAIL(QND_EUNSUPPORTED, "axis length %d: this build supports powers of two from 2 to 4096", L);
+    }
+#undef QND_CASE
+}
+
+enum ObsKind { OB_ZERO, OB_NORM, OB_DIPOLE_R, OB_ACCEL, OB_DIPOLE_V, OB_ENERGY, OB_LZ };
+
+struct ObsItem {
+    ObsKind kind;
+    int offset, width;
+};
+
+static const double MAX_EXP_ARG = 700.;  // integrators.h:12
+
+}  // namespace qnd
+
+using namespace qnd;
+
+struct qnd_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    bool fp64 = true;
+    int dim = 0;
+    int64_t nr[MAX_DIM] = {1, 1, 1};
+    double dr[MAX_DIM] = {0, 0, 0};
+    int64_t n = 0;
+    int lognr[MAX_DIM] = {0, 0, 0};
+    int shift[MAX_DIM] = {0, 0, 0};
+    std::string integrator;
+    double dt = 0;
+    int s = 0;
+    double as[20] = {0};
+    double dNr = 1, dNp = 1;
+    int axoff[MAX_DIM] = {0, 0, 0};
+    int axtot = 0;
+
+    std::vector<double> r[MAX_DIM], p[MAX_DIM];
+    std::vector<double> vpot, vcap;
+    std::vector<double> gradv[MAX_DIM];
+    std::vector<double> mask[MAX_DIM];
+    uint64_t table_epoch = 0;  // bumps when V / Vcap change; invalidates r-space tables
+
+    DevBuf tw[MAX_DIM];
+    DevBuf r_dev, p_dev;  // concatenated axes (double)
+    DevBuf gradv_dev[MAX_DIM];
+    DevBuf mask_dev[MAX_DIM];
+    DevBuf vpot_dev;      // double, for the energy operator
+    std::map<std::tuple<int, int, double, double>, std::unique_ptr<DevBuf>> spec_cache;
+    std::map<std::tuple<int, double, double, uint64_t>, std::unique_ptr<DevBuf>> rtab_cache;
+
+    DevBuf partials, counter, obs_dev, scal;  // reduction scratch; scal: [0]=gs norm2 [1]=gs scale [2..] coefs
+    DevBuf gs_flag;
+    DevBuf field_dev, field_tab, wtab_dev[MAX_DIM], spec_tmp[MAX_DIM];
+    DevBuf scratch_a, scratch_b;
+    std::vector<char> host_tmp;
+
+    bool profiling = false;
+    int64_t kernels_launched = 0;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pairs;
+    std::vector<cudaEvent_t> event_pool;
+
+    size_t elem() const { return fp64 ? 16 : 8; }
+    size_t rsize() const { return fp64 ? 8 : 4; }
+};
+
+namespace qnd {
+
+// ---------------------------------------------------------------- tables --
+
+// Twiddles of HostPlan(L) in the [j mod Ns][r-1] layout, exp(-2 pi i jm r / (Ns R)), in long double.
+static void build_twiddles(qnd_ctx* c, int ax) {
+    const int L = int(c->nr[ax]);
+    HostPlan pl(L);
+    std::vector<double> tw(2 * size_t(pl.tw_size > 0 ? pl.tw_size : 1));
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    size_t o = 0;
+    for (int st = 1; st < pl.nstage; ++st) {
+        const int R = pl.radix[st], Ns = pl.span[st];
+        for (int jm = 0; jm < Ns; ++jm)
+            for (int r = 1; r < R; ++r) {
+                long double ang = two_pi * (long double)(jm * r) / (long double)(Ns * R);
+                tw[2 * o] = (double)cosl(ang);
+                tw[2 * o + 1] = (double)(-sinl(ang));
+                ++o;
+            }
+    }
+    const size_t cnt = size_t(pl.tw_size > 0 ? pl.tw_size : 1);
+    c->tw[ax].ensure(cnt * c->elem());
+    if (c->fp64) {
+        QND_CK(cudaMemcpy(c->tw[ax].p, tw.data(), cnt * 16, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> f(2 * cnt);
+        for (size_t i = 0; i < 2 * cnt; ++i) f[i] = float(tw[i]);
+        QND_CK(cudaMemcpy(c->tw[ax].p, f.data(), cnt * 8, cudaMemcpyHostToDevice));
+    }
+}
+
+// Upload n complex values given as interleaved doubles, converting to the context precision.
+static void upload_cplx(qnd_ctx* c, DevBuf& dst, const std::vector<double>& v) {
+    const size_t n = v.size() / 2;
+    dst.ensure(n * c->elem());
+    if (c->fp64) {
+        QND_CK(cudaMemcpy(dst.p, v.data(), n * 16, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> f(2 * n);
+        for (size_t i = 0; i < 2 * n; ++i) {
+            f[i] = float(v[i]);
+            if (std::isinf(f[i]) && !std::isinf(v[i]))
+                QND_FAIL(QND_EUNSUPPORTED, "a phase/decay factor exceeds the FP32 range: use QND_FP64 for this case");
+        }
+        QND_CK(cudaMemcpy(dst.p, f.data(), n * 8, cudaMemcpyHostToDevice));
+    }
+}
+
+static void upload_real(qnd_ctx* c, DevBuf& dst, const std::vector<double>& v) {
+    const size_t n = v.size();
+    dst.ensure(n * c->rsize());
+    if (c->fp64) {
+        QND_CK(cudaMemcpy(dst.p, v.data(), n * 8, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<float> f(n);
+        for (size_t i = 0; i < n; ++i) {
+            f[i] = float(v[i]);
+            if (std::isinf(f[i]) && !std::isinf(v[i]))
+                QND_FAIL(QND_EUNSUPPORTED, "a decay factor exceeds the FP32 range: use QND_FP64 for this case");
+        }
+        QND_CK(cudaMemcpy(dst.p, f.data(), n * 4, cudaMemcpyHostToDevice));
+    }
+}
+
+static void upload_f64(DevBuf& dst, const std::vector<double>& v) {
+    dst.ensure(v.size() * 8);
+    QND_CK(cudaMemcpy(dst.p, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+}
+
+enum SpecKind { SP_LENGTH = 0, SP_IMAG = 1, SP_KIN = 2 };
+
+// Per-axis spectral factor tables (include the 1/N_axis of the inverse transform):
+//   SP_LENGTH: exp(-i c p^2/2)/N     (integrators.c:177, :192 factorised over axes)
+//   SP_IMAG:   exp(-c p^2/2)/N       (integrators.c:151-153; clamp checked up front)
+//   SP_KIN:    (p^2/2)/N             (the kinetic operator of calculate_observables.c:165)
+static const void* spec_table(qnd_ctx* c, int kind, int ax, double coef) {
+    auto key = std::make_tuple(kind, ax, coef, 0.0);
+    auto it = c->spec_cache.find(key);
+    if (it != c->spec_cache.end()) return it->second->p;
+    const int N = int(c->nr[ax]);
+    std::vector<double> v(2 * size_t(N));
+    for (int k = 0; k < N; ++k) {
+        const double pk = c->p[ax][k];
+        const double kin = .5 * pk * pk;
+        double re, im;
+        if (kind == SP_LENGTH) {
+            const double th = coef * kin;
+            re = std::cos(th) / N;
+            im = -std::sin(th) / N;
+        } else if (kind == SP_IMAG) {
+            re = std::exp(-coef * kin) / N;
+            im = 0;
+        } else {
+            re = kin / N;
+            im = 0;
+        }
+        v[2 * k] = re;
+        v[2 * k + 1] = im;
+    }
+    auto buf = std::make_unique<DevBuf>();
+    upload_cplx(c, *buf, v);
+    const void* ptr = buf->p;
+    c->spec_cache[key] = std::move(buf);
+    return ptr;
+}
+
+enum RtabKind { RT_IMAG = 0, RT_LENGTH = 1, RT_VEL = 2 };
+static const double NO_COEF = 1e300;  // marks "no second factor"
+
+static inline double clamped_exp(double arg) { return std::exp(arg > MAX_EXP_ARG ? MAX_EXP_ARG : arg); }
+
+// Full-grid r-space factor tables.
+//   RT_IMAG   (a[, b]):  exp(min(700, -a V)) [* exp(min(700, -b V))]           real (integrators.c:143-160)
+//   RT_LENGTH (h):       exp(min(700, -h Vcap)) exp(-i h V)                      complex (integrators.c:186-188)
+//   RT_VEL    (a[, b]):  exp(min(700,-a Vcap)) exp(-i a V) [* same with b]       complex (integrators.c:209-229)
+static const void* rtab(qnd_ctx* c, int kind, double a, double b) {
+    auto key = std::make_tuple(kind, a, b, c->table_epoch);
+    auto it = c->rtab_cache.find(key);
+    if (it != c->rtab_cache.end()) return it->second->p;
+    if (c->vpot.empty()) QND_FAIL(QND_EINVAL, "no potential set: call qnd_set_potential_named or qnd_set_potential");
+    const size_t n = size_t(c->n);
+    auto buf = std::make_unique<DevBuf>();
+    if (kind == RT_IMAG) {
+        std::vector<double> v(n);
+        for (size_t i = 0; i < n; ++i) {
+            double f = clamped_exp(-a * c->vpot[i]);
+            if (b != NO_COEF) f *= clamped_exp(-b * c->vpot[i]);
+            v[i] = f;
+        }
+        upload_real(c, *buf, v);
+    } else {
+        std::vector<double> v(2 * n);
+        for (size_t i = 0; i < n; ++i) {
+            const double vc = c->vcap.empty() ? 0.0 : c->vcap[i];
+            double re, im;
+            if (kind == RT_LENGTH) {
+                const double m = clamped_exp(-a * vc), th = a * c->vpot[i];
+                re = m * std::cos(th);
+                im = -m * std::sin(th);
+            } else {
+                const double m1 = clamped_exp(-a * vc), th1 = a * c->vpot[i];
+                re = m1 * std::cos(th1);
+                im = -m1 * std::sin(th1);
+                if (b != NO_COEF) {
+                    const double m2 = clamped_exp(-b * vc), th2 = b * c->vpot[i];
+                    const double r2 = m2 * std::cos(th2), i2 = -m2 * std::sin(th2);
+                    const double nr_ = re * r2 - im * i2, ni = re * i2 + im * r2;
+                    re = nr_;
+                    im = ni;
+                }
+            }
+            v[2 * i] = re;
+            v[2 * i + 1] = im;
+        }
+        upload_cplx(c, *buf, v);
+    }
+    const void* ptr = buf->p;
+    c->rtab_cache[key] = std::move(buf);
+    return ptr;
+}
+
+static void invalidate_rtabs(qnd_ctx* c) {
+    c->rtab_cache.clear();
+    c->table_epoch++;
+}
+
+// ---------------------------------------------------------------- passes --
+
+struct PassSpec {
+    int axis = 0;
+    int mode = PM_SANDWICH;
+    void* psi = nullptr;
+    void* dst = nullptr;
+    const void* partner = nullptr;
+    const void* pro_real = nullptr;
+    const void* pro_cplx = nullptr;
+    const double* pro_scale = nullptr;
+    const void* spec = nullptr;
+    const void* epi_real = nullptr;
+    const void* epi_cplx = nullptr;
+    const void* ax_cplx[MAX_DIM] = {nullptr, nullptr, nullptr};
+    const void* ax_real[MAX_DIM] = {nullptr, nullptr, nullptr};
+    double scale = 1.0;
+    int apply_acc = 0;
+    const double* apply_vtab = nullptr;
+    RedDesc red{};
+};
+
+static void ensure_red_scratch(qnd_ctx* c, long long blocks) {
+    const size_t need = size_t(blocks) * MAX_RED * sizeof(double);
+    if (c->partials.bytes < need) c->partials.ensure(need);
+    if (!c->counter.p) {
+        c->counter.ensure(64);
+        QND_CK(cudaMemset(c->counter.p, 0, 64));
+    }
+}
+
+template <typename R> static void fill_args(qnd_ctx* c, const PassSpec& ps, PassArgs<R>& a) {
+    using V = cplx_t<R>;
+    std::memset(&a, 0, sizeof a);
+    a.psi = static_cast<V*>(ps.psi);
+    a.dst = static_cast<V*>(ps.dst);
+    a.partner = static_cast<const V*>(ps.partner);
+    a.dim = c->dim;
+    for (int k = 0; k < MAX_DIM; ++k) {
+        a.shift[k] = c->shift[k];
+        a.nmask[k] = c->nr[k] - 1;
+    }
+    a.pro_real = static_cast<const R*>(ps.pro_real);
+    a.pro_cplx = static_cast<const V*>(ps.pro_cplx);
+    a.pro_scale_dev = ps.pro_scale;
+    a.spec = static_cast<const V*>(ps.spec);
+    a.epi_real = static_cast<const R*>(ps.epi_real);
+    a.epi_cplx = static_cast<const V*>(ps.epi_cplx);
+    for (int k = 0; k < MAX_DIM; ++k) {
+        a.ax_cplx[k] = static_cast<const V*>(ps.ax_cplx[k]);
+        a.ax_real[k] = static_cast<const R*>(ps.ax_real[k]);
+    }
+    a.scale = R(ps.scale);
+    a.apply_acc = ps.apply_acc;
+    a.apply_vtab = ps.apply_vtab;
+    a.red = ps.red;
+}
+
+static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
+    const int ax = ps.axis;
+    const int L = int(c->nr[ax]);
+    const int log2S = c->shift[ax];
+    const bool strided = log2S > 0;
+    const PassKernelInfo info = lookup_pass(c->fp64, L, strided, ps.mode);
+    const long long nlines = c->n / L;
+    const long long blocks = (nlines + info.G - 1) / info.G;
+    RedDesc red = ps.red;
+    if (red.n) {
+        ensure_red_scratch(c, blocks);
+        red.partials = c->partials.as<double>();
+        red.counter = c->counter.as<unsigned int>();
+    }
+    static std::map<std::pair<const void*, int>, bool> configured;  // per (kernel, device)
+    auto cfg_key = std::make_pair(info.fn, c->device);
+    if (!configured[cfg_key]) {
+        QND_CK(cudaFuncSetAttribute(info.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(info.smem)));
+        configured[cfg_key] = true;
+    }
+    std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
+    if (c->profiling) {
+        for (cudaEvent_t* e : {&ev.first, &ev.second}) {
+            if (c->event_pool.empty()) {
+                QND_CK(cudaEventCreate(e));
+            } else {
+                *e = c->event_pool.back();
+                c->event_pool.pop_back();
+            }
+        }
+        QND_CK(cudaEventRecord(ev.first, c->stream));
+    }
+    if (c->fp64) {
+        PassArgs<double> a;
+        fill_args<double>(c, ps, a);
+        a.red = red;
+        a.tw = c->tw[ax].as<double2>();
+        a.log2S = log2S;
+        a.nlines = nlines;
+        void* args[] = {&a};
+        QND_CK(cudaLaunchKernel(info.fn, dim3(unsigned(blocks)), dim3(info.nt), args, info.smem, c->stream));
+    } else {
+        PassArgs<float> a;
+        fill_args<float>(c, ps, a);
+        a.red = red;
+        a.tw = c->tw[ax].as<float2>();
+        a.log2S = log2S;
+        a.nlines = nlines;
+        void* args[] = {&a};
+        QND_CK(cudaLaunchKernel(info.fn, dim3(unsigned(blocks)), dim3(info.nt), args, info.smem, c->stream));
+    }
+    c->kernels_launched++;
+    if (c->profiling) {
+        QND_CK(cudaEventRecord(ev.second, c->stream));
+        c->prof_pairs.push_back(ev);
+    }
+}
+
+static int reduce_blocks(qnd_ctx* c) {
+    long long nb = (c->n + 255) / 256;
+    if (nb > 148 * 4) nb = 148 * 4;
+    return int(nb < 1 ? 1 : nb);
+}
+
+// Element-wise r-space reductions of psi.
+static void grid_reduce(qnd_ctx* c, const void* psi, const RedDesc& rd_in) {
+    RedDesc rd = rd_in;
+    const int nb = reduce_blocks(c);
+    ensure_red_scratch(c, nb);
+    rd.partials = c->partials.as<double>();
+    rd.counter = c->counter.as<unsigned int>();
+    PassSpec ps;
+    ps.psi = const_cast<void*>(psi);
+    ps.red = rd;
+    if (c->fp64) {
+        PassArgs<double> a;
+        fill_args<double>(c, ps, a);
+        launch_grid_reduce<double>(a, c->n, c->stream, nb);
+    } else {
+        PassArgs<float> a;
+        fill_args<float>(c, ps, a);
+        launch_grid_reduce<float>(a, c->n, c->stream, nb);
+    }
+    c->kernels_launched++;
+    QND_CK(cudaGetLastError());
+}
+
+// Axes in pass order: the contiguous axis first, axis 0 last (the last pass carries the epilogue).
+static std::vector<int> pass_order(const qnd_ctx* c) {
+    std::vector<int> o;
+    for (int k = c->dim - 1; k >= 0; --k) o.push_back(k);
+    return o;
+}
+
+// ---------------------------------------------------------------- observables --
+
+static std::vector<ObsItem> parse_obs(qnd_ctx* c, int nobs, const char* const* names, int* nvalues) {
+    std::vector<ObsItem> items;
+    int off = 0;
+    for (int k = 0; k < nobs; ++k) {
+        const char* nm = names[k] ? names[k] : "";
+        ObsItem it{OB_ZERO, off, 0};
+        if (!strcmp(nm, "norm")) it = {OB_NORM, off, 1};
+        else if (!strcmp(nm, "dipole_r")) it = {OB_DIPOLE_R, off, c->dim};
+        else if (!strcmp(nm, "accel")) it = {OB_ACCEL, off, c->dim};
+        else if (!strcmp(nm, "dipole_v")) it = {OB_DIPOLE_V, off, c->dim};
+        else if (!strcmp(nm, "energy")) it = {OB_ENERGY, off, 1};
+        else if (!strcmp(nm, "Lz")) it = {OB_LZ, off, 1};
+        if (it.kind == OB_ACCEL)
+            for (int j = 0; j < c->dim; ++j)
+                if (!c->gradv_dev[j].p) QND_FAIL(QND_EINVAL, "observable 'accel' needs qnd_set_gradv for every axis");
+        off += it.width;
+        items.push_back(it);
+    }
+    if (nvalues) *nvalues = off;
+    return items;
+}
+
+static bool all_rspace(const std::vector<ObsItem>& items) {
+    for (auto& it : items)
+        if (it.kind == OB_DIPOLE_V || it.kind == OB_ENERGY || it.kind == OB_LZ) return false;
+    return true;
+}
+
+// Reductions of |psi|^2 for the r-space observables, writing into row (the contiguous
+// outputs must be adjacent: r-space items are emitted in one descriptor per contiguous run).
+static std::vector<RedDesc> rspace_red(qnd_ctx* c, const std::vector<ObsItem>& items, double* row) {
+    std::vector<RedDesc> out;
+    RedDesc cur{};
+    int cur_off = -1;
+    auto flush = [&]() {
+        if (cur.n) out.push_back(cur);
+        cur = RedDesc{};
+        cur_off = -1;
+    };
+    auto add = [&](int off, int kind, int wkind, int waxis, const double* wtab, double scale) {
+        if (cur.n == MAX_RED || (cur.n && cur_off + cur.n != off)) flush();
+        if (!cur.n) {
+            cur_off = off;
+            cur.out = row + off;
+        }
+        cur.kind[cur.n] = kind;
+        cur.wkind[cur.n] = wkind;
+        cur.waxis[cur.n] = waxis;
+        cur.wtab[cur.n] = wtab;
+        cur.scale[cur.n] = scale;
+        cur.n++;
+    };
+    for (auto& it : items) {
+        if (it.kind == OB_NORM) add(it.offset, RK_ABS2, WK_ONE, 0, nullptr, c->dNr);
+        else if (it.kind == OB_DIPOLE_R)
+            for (int j = 0; j < c->dim; ++j) add(it.offset + j, RK_ABS2, WK_AXIS, j, c->r_dev.as<double>() + c->axoff[j], c->dNr);
+        else if (it.kind == OB_ACCEL)
+            for (int j = 0; j < c->dim; ++j) add(it.offset + j, RK_ABS2, WK_GRID, 0, c->gradv_dev[j].as<double>(), -c->dNr);
+    }
+    flush();
+    return out;
+}
+
+static void ensure_scratch_state(qnd_ctx* c, DevBuf& b) { b.ensure(size_t(c->n) * c->elem()); }
+
+static void ensure_vpot_dev(qnd_ctx* c) {
+    if (c->vpot.empty()) QND_FAIL(QND_EINVAL, "no potential set");
+    if (!c->vpot_dev.p) upload_f64(c->vpot_dev, c->vpot);
+}
+
+// out[m-1] = Re <psi | H^m | psi> dNr for m = 1..nmom (calculate_observables.c:146-175), written to dev.
+static void energy_moments(qnd_ctx* c, const void* psi, int nmom, double* out_dev) {
+    ensure_vpot_dev(c);
+    ensure_scratch_state(c, c->scratch_a);
+    if (nmom > 1) ensure_scratch_state(c, c->scratch_b);
+    const void* src = psi;
+    auto order = pass_order(c);
+    for (int m = 1; m <= nmom; ++m) {
+        void* dst = (m % 2) ? c->scratch_a.p : c->scratch_b.p;
+        for (size_t q = 0; q < order.size(); ++q) {
+            const int ax = order[q];
+            PassSpec ps;
+            ps.axis = ax;
+            ps.mode = PM_APPLY;
+            ps.psi = const_cast<void*>(src);
+            ps.dst = dst;
+            ps.spec = spec_table(c, SP_KIN, ax, 0.0);
+            if (q == 0) ps.apply_vtab = c->vpot_dev.as<double>();
+            else ps.apply_acc = 1;
+            if (q + 1 == order.size()) {
+                ps.partner = psi;
+                ps.red.n = 1;
+                ps.red.kind[0] = RK_BILIN;
+                ps.red.wkind[0] = WK_ONE;
+                ps.red.scale[0] = c->dNr;
+                ps.red.out = out_dev + (m - 1);
+            }
+            launch_pass(c, ps);
+        }
+        src = dst;
+    }
+}
+
+// Evaluate observables of an r-space psi into the device row (calculate_observables.c:119-140).
+static void eval_obs(qnd_ctx* c, const void* psi, const std::vector<ObsItem>& items, const double* alpha,
+                     double* row_dev) {
+    for (auto& rd : rspace_red(c, items, row_dev)) grid_reduce(c, psi, rd);
+    for (auto& it : items) {
+        if (it.kind == OB_DIPOLE_V) {
+            // sum_k |psi~|^2 (p_j + alpha_j) dNp fft_scaling = (dNp/N_j) sum |F_j psi|^2 (p_j + alpha_j)
+            for (int j = 0; j < c->dim; ++j) {
+                c->wtab_dev[j].ensure(size_t(c->nr[j]) * 8);
+                if (c->fp64)
+                    launch_axis_table<double>(0, c->p_dev.as<double>() + c->axoff[j], int(c->nr[j]), alpha[j],
+                                              c->wtab_dev[j].p, c->stream);
+                else
+                    launch_axis_table<float>(0, c->p_dev.as<double>() + c->axoff[j], int(c->nr[j]), alpha[j],
+                                             c->wtab_dev[j].p, c->stream);
+                c->kernels_launched++;
+                PassSpec ps;
+                ps.axis = j;
+                ps.mode = PM_SPECRED;
+                ps.psi = const_cast<void*>(psi);
+                ps.red.n = 1;
+                ps.red.kind[0] = RK_ABS2;
+                ps.red.wkind[0] = WK_AXIS;
+                ps.red.waxis[0] = j;
+                ps.red.wtab[0] = c->wtab_dev[j].as<double>();
+                ps.red.scale[0] = c->dNp / double(c->nr[j]);
+                ps.red.out = row_dev + it.offset + j;
+                launch_pass(c, ps);
+            }
+        } else if (it.kind == OB_ENERGY) {
+            energy_moments(c, psi, 1, row_dev + it.offset);
+        } else if (it.kind == OB_LZ) {
+            if (c->dim <= 1) {
+                QND_CK(cudaMemsetAsync(row_dev + it.offset, 0, sizeof(double), c->stream));
+                continue;
+            }
+            // Lz = Re sum conj(psi) [x T'_y psi - y T'_x psi] dNr, T'_j = F_j^-1 (p_j + A_j) F_j / N_j
+            for (int q = 0; q < 2; ++q) {
+                const int opax = q == 0 ? 1 : 0, wax = q == 0 ? 0 : 1;
+                c->spec_tmp[opax].ensure(size_t(c->nr[opax]) * c->elem());
+                if (c->fp64)
+                    launch_axis_table<double>(1, c->p_dev.as<double>() + c->axoff[opax], int(c->nr[opax]),
+                                              alpha[opax], c->spec_tmp[opax].p, c->stream);
+                else
+                    launch_axis_table<float>(1, c->p_dev.as<double>() + c->axoff[opax], int(c->nr[opax]),
+                                             alpha[opax], c->spec_tmp[opax].p, c->stream);
+                c->kernels_launched++;
+                PassSpec ps;
+                ps.axis = opax;
+                ps.mode = PM_APPLY;
+                ps.psi = const_cast<void*>(psi);
+                ps.spec = c->spec_tmp[opax].p;
+                ps.partner = psi;
+                ps.red.n = 1;
+                ps.red.kind[0] = RK_BILIN;
+                ps.red.wkind[0] = WK_AXIS;
+                ps.red.waxis[0] = wax;
+                ps.red.wtab[0] = c->r_dev.as<double>() + c->axoff[wax];
+                ps.red.scale[0] = q == 0 ? c->dNr : -c->dNr;
+                ps.red.accumulate = q;
+                ps.red.out = row_dev + it.offset;
+                launch_pass(c, ps);
+            }
+        } else if (it.kind == OB_ZERO && it.width) {
+            QND_CK(cudaMemsetAsync(row_dev + it.offset, 0, it.width * sizeof(double), c->stream));
+        }
+    }
+}
+
+// ---------------------------------------------------------------- steps --
+
+static void check_imag_clamp(qnd_ctx* c) {
+    // The per-axis factorisation of exp(min(700, -c Kin)) is exact unless the clamp engages.
+    double kmax = 0;
+    for (int j = 0; j < c->dim; ++j) {
+        double m = 0;
+        for (double pk : c->p[j]) m = std::max(m, .5 * pk * pk);
+        kmax += m;
+    }
+    for (int ia = 0; ia < c->s; ++ia) {
+        const double h = c->as[2 * ia] + c->as[2 * ia + 1];
+        if (-h * kmax > MAX_EXP_ARG)
+            QND_FAIL(QND_EUNSUPPORTED,
+                     "imaginary-time kinetic factor reaches the exp(700) clamp (dt too large for this grid)");
+    }
+}
+
+// Integration_step_imag x nsteps on an r-space psi (integrators.c:135-163). pro_scale (device scalar,
+// may be null) multiplies psi before the first step (deferred Gram-Schmidt normalisation).
+static void imag_steps(qnd_ctx* c, void* psi, int64_t nsteps, const double* pro_scale) {
+    check_imag_clamp(c);
+    auto order = pass_order(c);
+    for (int64_t st = 0; st < nsteps; ++st) {
+        for (int ia = 0; ia < c->s; ++ia) {
+            const double a = c->as[2 * ia], b = c->as[2 * ia + 1], h = a + b;
+            for (size_t q = 0; q < order.size(); ++q) {
+                PassSpec ps;
+                ps.axis = order[q];
+                ps.psi = psi;
+                ps.spec = spec_table(c, SP_IMAG, order[q], h);
+                if (q == 0 && ia == 0) {
+                    ps.pro_real = rtab(c, RT_IMAG, a, NO_COEF);
+                    if (st == 0) ps.pro_scale = pro_scale;
+                }
+                if (q + 1 == order.size())
+                    ps.epi_real = ia + 1 < c->s ? rtab(c, RT_IMAG, b, c->as[2 * ia + 2]) : rtab(c, RT_IMAG, b, NO_COEF);
+                launch_pass(c, ps);
+            }
+        }
+    }
+}
+
+// Per-step field tables (laser phases / velocity-gauge kinetic phases) for a chunk of steps
+// from field samples already on the device.
+static void build_field_tables(qnd_ctx* c, const double* field_dev, int64_t nsteps, bool velocity) {
+    FieldTableArgs fa{};
+    fa.field = field_dev;
+    fa.axes = velocity ? c->p_dev.as<double>() : c->r_dev.as<double>();
+    fa.nsteps = int(nsteps);
+    fa.s = c->s;
+    fa.dim = c->dim;
+    for (int j = 0; j < c->dim; ++j) {
+        fa.nr[j] = int(c->nr[j]);
+        fa.off[j] = c->axoff[j];
+    }
+    fa.ntot = c->axtot;
+    for (int ia = 0; ia < c->s; ++ia) fa.h[ia] = c->as[2 * ia] + c->as[2 * ia + 1];
+    fa.velocity = velocity ? 1 : 0;
+    c->field_tab.ensure(size_t(nsteps) * c->s * c->axtot * c->elem());
+    if (c->fp64) launch_field_tables<double>(fa, c->field_tab.as<double2>(), c->stream);
+    else launch_field_tables<float>(fa, c->field_tab.as<float2>(), c->stream);
+    c->kernels_launched++;
+    QND_CK(cudaGetLastError());
+}
+
+static void upload_field_chunk(qnd_ctx* c, const double* host, int64_t nsteps, bool velocity) {
+    const size_t nval = size_t(nsteps) * c->s * c->dim;
+    c->field_dev.ensure(nval * 8);
+    QND_CK(cudaMemcpyAsync(c->field_dev.p, host, nval * 8, cudaMemcpyHostToDevice, c->stream));
+    build_field_tables(c, c->field_dev.as<double>(), nsteps, velocity);
+}
+
+static const void* field_slice(qnd_ctx* c, int64_t st, int ia, int ax) {
+    const size_t idx = (size_t(st) * c->s + ia) * c->axtot + c->axoff[ax];
+    return static_cast<const char*>(c->field_tab.p) + idx * c->elem();
+}
+
+static bool has_mask(const qnd_ctx* c) {
+    for (int j = 0; j < c->dim; ++j)
+        if (c->mask_dev[j].p) return true;
+    return false;
+}
+
+// One length-gauge step in r-space (chunk-local step index lst for the field tables).
+// fin: reductions fused into the final pass (may have n == 0); masked: apply the step mask.
+static void length_step(qnd_ctx* c, void* psi, int64_t lst, const std::vector<RedDesc>& fin, bool masked) {
+    auto order = pass_order(c);
+    for (int ia = 0; ia <= c->s; ++ia) {
+        // kinetic sandwich before V(h_ia): K(a_0) first, K(a_{2ia-1} + a_{2ia}) between, K(a_{2s-1}) last
+        double kc;
+        if (ia == 0) kc = c->as[0];
+        else if (ia == c->s) kc = c->as[2 * c->s - 1];
+        else kc = c->as[2 * ia - 1] + c->as[2 * ia];
+        for (size_t q = 0; q < order.size(); ++q) {
+            PassSpec ps;
+            ps.axis = order[q];
+            ps.psi = psi;
+            ps.spec = spec_table(c, SP_LENGTH, order[q], kc);
+            if (q + 1 == order.size()) {
+                if (ia < c->s) {
+                    const double h = c->as[2 * ia] + c->as[2 * ia + 1];
+                    ps.epi_cplx = rtab(c, RT_LENGTH, h, NO_COEF);
+                    for (int j = 0; j < c->dim; ++j) ps.ax_cplx[j] = field_slice(c, lst, ia, j);
+                } else {
+                    if (masked)
+                        for (int j = 0; j < c->dim; ++j) ps.ax_real[j] = c->mask_dev[j].p;
+                    if (!fin.empty()) ps.red = fin[0];
+                }
+            }
+            launch_pass(c, ps);
+        }
+    }
+    // further reduction descriptors (more than one run of outputs) read the final state again
+    for (size_t k = 1; k < fin.size(); ++k) grid_reduce(c, psi, fin[k]);
+}
+
+// One velocity-gauge step in r-space (integrators.c:201-232).
+static void velocity_step(qnd_ctx* c, void* psi, int64_t lst, const std::vector<RedDesc>& fin, bool masked) {
+    auto order = pass_order(c);
+    for (int ia = 0; ia < c->s; ++ia) {
+        const double a = c->as[2 * ia], b = c->as[2 * ia + 1];
+        for (size_t q = 0; q < order.size(); ++q) {
+            PassSpec ps;
+            ps.axis = order[q];
+            ps.psi = psi;
+            ps.spec = field_slice(c, lst, ia, order[q]);
+            if (q == 0 && ia == 0) ps.pro_cplx = rtab(c, RT_VEL, a, NO_COEF);
+            if (q + 1 == order.size()) {
+                if (ia + 1 < c->s) {
+                    ps.epi_cplx = rtab(c, RT_VEL, b, c->as[2 * ia + 2]);
+                } else {
+                    ps.epi_cplx = rtab(c, RT_VEL, b, NO_COEF);
+                    if (masked)
+                        for (int j = 0; j < c->dim; ++j) ps.ax_real[j] = c->mask_dev[j].p;
+                    if (!fin.empty()) ps.red = fin[0];
+                }
+            }
+            launch_pass(c, ps);
+        }
+    }
+    for (size_t k = 1; k < fin.size(); ++k) grid_reduce(c, psi, fin[k]);
+}
+
+static void unitary_fft(qnd_ctx* c, void* psi, bool forward) {
+    for (int ax : pass_order(c)) {
+        PassSpec ps;
+        ps.axis = ax;
+        ps.mode = forward ? PM_FFT_FWD : PM_FFT_INV;
+        ps.psi = psi;
+        ps.scale = 1.0 / std::sqrt(double(c->nr[ax]));
+        launch_pass(c, ps);
+    }
+}
+
+static const int64_t CHUNK = 128;
+
+// Real-time driver loop (QuantumND_real.c:168-229) for either gauge.
+static void run_realtime(qnd_ctx* c, void* psi, const double* field_host, const double* alpha_host, int64_t nsteps,
+                         int nobs, const char* const* names, double* obs_host, bool velocity) {
+    int nv = 0;
+    auto items = parse_obs(c, nobs, names, &nv);
+    const bool fused = all_rspace(items) && !velocity;  // velocity obs use A(t) -> evaluate per step
+    const bool fused_v = all_rspace(items) && velocity;
+    const bool masked = has_mask(c);
+    const int64_t ch_max = std::min<int64_t>(CHUNK, std::max<int64_t>(nsteps, 1));
+    if (nv > 0) {
+        c->obs_dev.ensure(size_t(ch_max + 1) * nv * sizeof(double));
+        QND_CK(cudaMemsetAsync(c->obs_dev.p, 0, size_t(ch_max + 1) * nv * sizeof(double), c->stream));
+    }
+    std::vector<double> zero_alpha(MAX_DIM, 0.0);
+    double* rows = c->obs_dev.as<double>();
+    for (int64_t c0 = 0; c0 < nsteps; c0 += ch_max) {
+        const int64_t ch = std::min(ch_max, nsteps - c0);
+        if (nv > 0 && c0 == 0) {
+            const double* al = velocity ? alpha_host : zero_alpha.data();
+            eval_obs(c, psi, items, al, rows);
+        }
+        upload_field_chunk(c, field_host + size_t(c0) * c->s * c->dim, ch, velocity);
+        for (int64_t k = 0; k < ch; ++k) {
+            const int64_t gst = c0 + k;
+            double* row = rows + size_t(k + 1) * nv;
+            std::vector<RedDesc> fin;
+            if (nv > 0 && (fused || fused_v)) fin = rspace_red(c, items, row);
+            if (velocity) velocity_step(c, psi, k, fin, masked);
+            else length_step(c, psi, k, fin, masked);
+            if (nv > 0 && !(fused || fused_v) && gst + 1 < nsteps) {
+                const double* al = velocity ? alpha_host + size_t(gst + 1) * c->dim : zero_alpha.data();
+                eval_obs(c, psi, items, al, row);
+            }
+        }
+        if (nv > 0) {
+            // rows[0] holds obs(psi(t_c0)); rows[k+1] obs after step c0+k
+            const int64_t first = c0;  // host row index of rows[0]
+            const int64_t cnt = std::min<int64_t>(ch, nsteps - first);
+            QND_CK(cudaMemcpyAsync(obs_host + size_t(first) * nv, rows, size_t(cnt) * nv * sizeof(double),
+                                   cudaMemcpyDeviceToHost, c->stream));
+            QND_CK(cudaStreamSynchronize(c->stream));
+            // carry the last row (obs after the chunk) to the front for the next chunk
+            QND_CK(cudaMemcpyAsync(rows, rows + size_t(ch) * nv, nv * sizeof(double), cudaMemcpyDeviceToDevice,
+                                   c->stream));
+        }
+    }
+    QND_CK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------- Gram-Schmidt --
+
+// v = psi_j - sum_k <psi_k|psi_j> psi_k; norm2 = ||v||^2 dNr into scal[0]; scale 1/sqrt(norm2) into
+// scal[1]; the flag is raised when norm2 < 1e-12 (QuantumND_imag.c:280-304). The normalisation itself
+// is left to the caller (scale kernel or the next step's prologue).
+static void gs_project(qnd_ctx* c, void* const* states, int j) {
+    if (j >= GS_MAXK) QND_FAIL(QND_EUNSUPPORTED, "Gram-Schmidt against %d states (max %d)", j, GS_MAXK - 1);
+    c->scal.ensure(sizeof(double) * (2 + 2 * GS_MAXK));
+    if (!c->gs_flag.p) {
+        c->gs_flag.ensure(sizeof(int));
+        QND_CK(cudaMemsetAsync(c->gs_flag.p, 0, sizeof(int), c->stream));
+    }
+    double* scal = c->scal.as<double>();
+    const int nb = reduce_blocks(c);
+    ensure_red_scratch(c, nb);
+    auto run = [&](auto tag) {
+        using R = decltype(tag);
+        GSArgs<R> g;
+        std::memset(&g, 0, sizeof g);
+        g.psi = static_cast<cplx_t<R>*>(states[j]);
+        for (int k = 0; k < j; ++k) g.states[k] = static_cast<const cplx_t<R>*>(states[k]);
+        g.n = c->n;
+        g.red.partials = c->partials.as<double>();
+        g.red.counter = c->counter.as<unsigned int>();
+        for (int k0 = 0; k0 < j; k0 += MAX_RED / 2) {
+            g.k0 = k0;
+            g.nk = std::min(MAX_RED / 2, j - k0);
+            g.red.n = 2 * g.nk;
+            for (int q = 0; q < g.red.n; ++q) {
+                g.red.kind[q] = RK_ABS2;
+                g.red.wkind[q] = WK_ONE;
+                g.red.scale[q] = c->dNr;
+            }
+            g.red.out = scal + 2 + 2 * k0;
+            launch_gs_dot<R>(g, c->stream, nb);
+            c->kernels_launched++;
+        }
+        g.j = j;
+        g.coef = scal + 2;
+        g.red.n = 1;
+        g.red.scale[0] = c->dNr;
+        g.red.out = scal;
+        launch_gs_axpy<R>(g, c->stream, nb);
+        c->kernels_launched++;
+    };
+    if (c->fp64) run(double{});
+    else run(float{});
+    QND_CK(cudaGetLastError());
+    launch_gs_finalize(scal, 1.e-12, scal + 1, c->gs_flag.as<int>(), c->stream);
+    c->kernels_launched++;
+}
+
+static void check_gs_flag(qnd_ctx* c, int j) {
+    int flag = 0;
+    QND_CK(cudaMemcpyAsync(&flag, c->gs_flag.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    QND_CK(cudaStreamSynchronize(c->stream));
+    if (flag) {
+        QND_CK(cudaMemsetAsync(c->gs_flag.p, 0, sizeof(int), c->stream));
+        QND_FAIL(QND_ENORM, "Wavefunction norm decayed to zero during Gram-Schmidt for state %d (norm < 1e-12)", j);
+    }
+}
+
+static void scale_state(qnd_ctx* c, void* psi, const double* scale_dev) {
+    if (c->fp64) launch_scale<double>(static_cast<double2*>(psi), c->n, scale_dev, c->stream);
+    else launch_scale<float>(static_cast<float2*>(psi), c->n, scale_dev, c->stream);
+    c->kernels_launched++;
+    QND_CK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------- context --
+
+static void set_device(qnd_ctx* c) { QND_CK(cudaSetDevice(c->device)); }
+
+static void build_context(qnd_ctx* c, int dim, const int64_t* nr, const double* dr, const char* integrator,
+                          double dt, int precision) {
+    if (dim < 1 || dim > MAX_DIM) QND_FAIL(QND_EINVAL, "dimension %d not in 1..3", dim);
+    if (precision != QND_FP64 && precision != QND_MIXED) QND_FAIL(QND_EINVAL, "unknown precision %d", precision);
+    c->fp64 = precision == QND_FP64;
+    c->dim = dim;
+    c->n = 1;
+    for (int j = 0; j < dim; ++j) {
+        if (nr[j] < 2 || nr[j] > 4096 || (nr[j] & (nr[j] - 1)))
+            QND_FAIL(nr[j] > 4096 ? QND_EUNSUPPORTED : QND_EINVAL,
+                     "NR[%d]=%lld: must be a power of 2 between 2 and 4096", j, (long long)nr[j]);
+        if (!(dr[j] > 0)) QND_FAIL(QND_EINVAL, "DR[%d] must be positive", j);
+        c->nr[j] = nr[j];
+        c->dr[j] = dr[j];
+        c->n *= nr[j];
+        int l = 0;
+        while ((int64_t(1) << l) < nr[j]) ++l;
+        c->lognr[j] = l;
+    }
+    for (int j = 0; j < dim; ++j) {
+        int sh = 0;
+        for (int k = j + 1; k < dim; ++k) sh += c->lognr[k];
+        c->shift[j] = sh;
+    }
+    // integrator coefficients (integrators.c:22-64)
+    static const double verlet[] = {.5};
+    static const double bm4[] = {.0792036964311957, .1303114101821663, .2228614958676077,
+                                 -.3667132690474257, .3246481886897062, .1096884778767498};
+    static const double bm6[] = {.050262764400392, .098553683500650, .314960616927694, -.447346482695478,
+                                 .492426372489876, -.425118767797691, .237063913978122, .195602488600053,
+                                 .346358189850727, -.362762779254345};
+    static const double rkn4[] = {.082984406417405, .162314550766866, .233995250731502,
+                                  .370877414979578, -.409933719901926, .059762097006575};
+    const double* base = nullptr;
+    if (!integrator) QND_FAIL(QND_EINVAL, "integrator name is NULL");
+    if (!strcmp(integrator, "Verlet")) { base = verlet; c->s = 1; }
+    else if (!strcmp(integrator, "BM4")) { base = bm4; c->s = 6; }
+    else if (!strcmp(integrator, "BM6")) { base = bm6; c->s = 10; }
+    else if (!strcmp(integrator, "RKN4")) { base = rkn4; c->s = 6; }
+    else QND_FAIL(QND_EINVAL, "Unknown integrator: %s", integrator);
+    double as[20];
+    for (int j = 0; j < c->s; ++j) as[j] = base[j];
+    for (int j = 0; j < c->s; ++j) as[c->s + j] = as[c->s - 1 - j];
+    for (int j = 0; j < 2 * c->s; ++j) c->as[j] = as[j] * dt;
+    c->integrator = integrator;
+    c->dt = dt;
+    // grid (meshgrid.c:22-28, 75-89)
+    c->dNr = 1.;
+    c->dNp = 1.;
+    int off = 0;
+    for (int j = 0; j < dim; ++j) {
+        c->dNr *= dr[j];
+        c->dNp *= 2. * M_PI / (double)(dr[j] * nr[j]);
+        const int64_t N = nr[j];
+        const double L = dr[j] * N, dp = 2. * M_PI / L;
+        c->r[j].resize(N);
+        c->p[j].resize(N);
+        for (int64_t i = 0; i < N; ++i) {
+            c->r[j][i] = -.5 * L + i * dr[j];
+            c->p[j][i] = i < N / 2 ? i * dp : (i - N) * dp;
+        }
+        c->axoff[j] = off;
+        off += int(N);
+    }
+    c->axtot = off;
+    QND_CK(cudaGetDevice(&c->device));
+    QND_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->own_stream = true;
+    std::vector<double> rall, pall;
+    for (int j = 0; j < dim; ++j) {
+        rall.insert(rall.end(), c->r[j].begin(), c->r[j].end());
+        pall.insert(pall.end(), c->p[j].begin(), c->p[j].end());
+    }
+    upload_f64(c->r_dev, rall);
+    upload_f64(c->p_dev, pall);
+    for (int j = 0; j < dim; ++j) build_twiddles(c, j);
+}
+
+// Named potentials as functions of |r| (meshgrid.c:137-153) and their radial derivative dV/dr.
+static bool named_potential(const char* name, double r, double* v) {
+    const double r2 = r * r;
+    if (!strcmp(name, "H_1D")) *v = -1. / (double)sqrt(r2 + 2.);
+    else if (!strcmp(name, "H_3D")) *v = -1. / (double)sqrt(r2 + 1e-4);
+    else if (!strcmp(name, "H_2D")) *v = -1. / (double)sqrt(r2 + .7396);
+    else if (!strcmp(name, "Ne_2D")) *v = -(1. + 9. * exp(-r2)) / (double)sqrt(r2 + 2.88172);
+    else if (!strcmp(name, "Ar_2D")) *v = -(1. + 17. * exp(-r2)) / (double)sqrt(r2 + .91205);
+    else if (!strcmp(name, "Kr_2D")) *v = -(1. + 35. * exp(-r2)) / (double)sqrt(r2 + .7875);
+    else if (!strcmp(name, "Xe_2D")) *v = -(1. + 53. * exp(-r2)) / (double)sqrt(r2 + .52592);
+    else if (!strcmp(name, "Ne_short_2D")) *v = -2.7459 * exp(-.5 * r2 / 1.96);
+    else return false;
+    return true;
+}
+
+}  // namespace qnd
+
+// ================================================================ C API ==
+
+#define QND_API_BEGIN try {
+#define QND_API_END                                                   \
+    return QND_OK;                                                    \
+    }                                                                 \
+    catch (const ::qnd::Error& e) {                                   \
+        ::qnd::g_err = e.msg;                                         \
+        return e.code;                                                \
+    }                                                                 \
+    catch (const std::exception& e) {                                 \
+        ::qnd::g_err = e.what();                                      \
+        return QND_EINVAL;                                            \
+    }
+
+#define QND_NEED(ptr)                                                  \
+    if (!(ptr)) QND_FAIL(QND_EINVAL, "%s: %s is NULL", __func__, #ptr)
+
+extern "C" {
+
+const char* qnd_version(void) { return "qnd_b200 0.1 (sm_100a)"; }
+const char* qnd_last_error(void) { return qnd::g_err.c_str(); }
+
+int qnd_ctx_create(int dim, const int64_t* nr, const double* dr, const char* integrator, double dt, int precision,
+                   qnd_ctx** out) {
+    QND_API_BEGIN
+    QND_NEED(out);
+    QND_NEED(nr);
+    QND_NEED(dr);
+    *out = nullptr;
+    auto c = std::make_unique<qnd_ctx>();
+    build_context(c.get(), dim, nr, dr, integrator, dt, precision);
+    *out = c.release();
+    QND_API_END
+}
+
+int qnd_ctx_destroy(qnd_ctx* ctx) {
+    QND_API_BEGIN
+    if (!ctx) return QND_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& pr : ctx->prof_pairs) {
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+    }
+    for (auto e : ctx->event_pool) cudaEventDestroy(e);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    QND_API_END
+}
+
+int qnd_ctx_set_stream(qnd_ctx* ctx, void* stream) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    set_device(ctx);
+    QND_CK(cudaStreamSynchronize(ctx->stream));
+    if (stream) {
+        if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+        ctx->stream = static_cast<cudaStream_t>(stream);
+        ctx->own_stream = false;
+    } else if (!ctx->own_stream) {
+        QND_CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        ctx->own_stream = true;
+    }
+    QND_API_END
+}
+
+int qnd_ctx_info(qnd_ctx* ctx, int64_t* n_total, int* s_integrator, double* as_scaled, double* dNr, double* dNp) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    if (n_total) *n_total = ctx->n;
+    if (s_integrator) *s_integrator = ctx->s;
+    if (as_scaled)
+        for (int j = 0; j < 2 * ctx->s; ++j) as_scaled[j] = ctx->as[j];
+    if (dNr) *dNr = ctx->dNr;
+    if (dNp) *dNp = ctx->dNp;
+    QND_API_END
+}
+
+int qnd_state_bytes(qnd_ctx* ctx, int64_t* bytes) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(bytes);
+    *bytes = int64_t(ctx->n) * int64_t(ctx->elem());
+    QND_API_END
+}
+
+int qnd_set_potential_named(qnd_ctx* ctx, const char* name) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(name);
+    double probe;
+    if (!named_potential(name, 0.0, &probe)) QND_FAIL(QND_EINVAL, "Unknown potential: %s", name);
+    std::vector<double> v(size_t(ctx->n));
+    int64_t idx[MAX_DIM];
+    for (int64_t i = 0; i < ctx->n; ++i) {
+        int64_t rem = i;
+        for (int j = ctx->dim - 1; j >= 0; --j) {
+            idx[j] = rem % ctx->nr[j];
+            rem /= ctx->nr[j];
+        }
+        double r = 0.;
+        for (int j = 0; j < ctx->dim; ++j) {
+            const double x = ctx->r[j][idx[j]];
+            r += x * x;
+        }
+        r = sqrt(r);
+        named_potential(name, r, &v[size_t(i)]);
+    }
+    ctx->vpot.swap(v);
+    ctx->vpot_dev.reset();
+    invalidate_rtabs(ctx);
+    QND_API_END
+}
+
+int qnd_set_potential(qnd_ctx* ctx, const double* vpot_host) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(vpot_host);
+    ctx->vpot.assign(vpot_host, vpot_host + ctx->n);
+    ctx->vpot_dev.reset();
+    invalidate_rtabs(ctx);
+    QND_API_END
+}
+
+int qnd_set_cap(qnd_ctx* ctx, double strength, double length) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    std::vector<double> v(size_t(ctx->n), 0.0);
+    int64_t idx[MAX_DIM];
+    for (int64_t i = 0; i < ctx->n; ++i) {
+        int64_t rem = i;
+        for (int j = ctx->dim - 1; j >= 0; --j) {
+            idx[j] = rem % ctx->nr[j];
+            rem /= ctx->nr[j];
+        }
+        double acc = 0.;
+        for (int j = 0; j < ctx->dim; ++j) {
+            const double x = ctx->r[j][idx[j]];
+            const double L = .5 * ctx->nr[j] * ctx->dr[j] - length;
+            if (fabs(x) >= L) acc += strength * (fabs(x) - L) * (fabs(x) - L);
+        }
+        v[size_t(i)] = acc;
+    }
+    ctx->vcap.swap(v);
+    invalidate_rtabs(ctx);
+    QND_API_END
+}
+
+int qnd_set_vcap(qnd_ctx* ctx, const double* vcap_host) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    if (vcap_host) ctx->vcap.assign(vcap_host, vcap_host + ctx->n);
+    else ctx->vcap.clear();
+    invalidate_rtabs(ctx);
+    QND_API_END
+}
+
+int qnd_set_gradv(qnd_ctx* ctx, int axis, const double* gradv_host) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    if (axis < 0 || axis >= ctx->dim) QND_FAIL(QND_EINVAL, "axis %d out of range", axis);
+    set_device(ctx);
+    if (!gradv_host) {
+        ctx->gradv[axis].clear();
+        ctx->gradv_dev[axis].reset();
+    } else {
+        ctx->gradv[axis].assign(gradv_host, gradv_host + ctx->n);
+        upload_f64(ctx->gradv_dev[axis], ctx->gradv[axis]);
+    }
+    QND_API_END
+}
+
+int qnd_set_mask_axis(qnd_ctx* ctx, int axis, const double* mask_host) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    if (axis < 0 || axis >= ctx->dim) QND_FAIL(QND_EINVAL, "axis %d out of range", axis);
+    set_device(ctx);
+    if (!mask_host) {
+        ctx->mask[axis].clear();
+        ctx->mask_dev[axis].reset();
+    } else {
+        ctx->mask[axis].assign(mask_host, mask_host + ctx->nr[axis]);
+        upload_real(ctx, ctx->mask_dev[axis], ctx->mask[axis]);
+    }
+    QND_API_END
+}
+
+int qnd_state_alloc(qnd_ctx* ctx, int64_t nstates, void** psi_dev) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_dev);
+    if (nstates < 1) QND_FAIL(QND_EINVAL, "nstates must be >= 1");
+    set_device(ctx);
+    void* p = nullptr;
+    const size_t bytes = size_t(nstates) * size_t(ctx->n) * ctx->elem();
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        QND_FAIL(QND_ENOMEM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+    }
+    QND_CK(cudaMemsetAsync(p, 0, bytes, ctx->stream));
+    *psi_dev = p;
+    QND_API_END
+}
+
+int qnd_state_free(qnd_ctx* ctx, void* psi_dev) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    set_device(ctx);
+    QND_CK(cudaStreamSynchronize(ctx->stream));
+    if (psi_dev) QND_CK(cudaFree(psi_dev));
+    QND_API_END
+}
+
+int qnd_state_upload(qnd_ctx* ctx, void* psi_dev, const double* host) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_dev);
+    QND_NEED(host);
+    set_device(ctx);
+    if (ctx->fp64) {
+        QND_CK(cudaMemcpyAsync(psi_dev, host, size_t(ctx->n) * 16, cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+        ctx->host_tmp.resize(size_t(ctx->n) * 8);
+        float* f = reinterpret_cast<float*>(ctx->host_tmp.data());
+        QND_CK(cudaStreamSynchronize(ctx->stream));
+        for (int64_t i = 0; i < 2 * ctx->n; ++i) f[i] = float(host[i]);
+        QND_CK(cudaMemcpyAsync(psi_dev, f, size_t(ctx->n) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    }
+    QND_CK(cudaStreamSynchronize(ctx->stream));
+    QND_API_END
+}
+
+int qnd_state_download(qnd_ctx* ctx, double* host, const void* psi_dev) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_dev);
+    QND_NEED(host);
+    set_device(ctx);
+    if (ctx->fp64) {
+        QND_CK(cudaMemcpyAsync(host, psi_dev, size_t(ctx->n) * 16, cudaMemcpyDeviceToHost, ctx->stream));
+        QND_CK(cudaStreamSynchronize(ctx->stream));
+    } else {
+        ctx->host_tmp.resize(size_t(ctx->n) * 8);
+        float* f = reinterpret_cast<float*>(ctx->host_tmp.data());
+        QND_CK(cudaMemcpyAsync(f, psi_dev, size_t(ctx->n) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        QND_CK(cudaStreamSynchronize(ctx->stream));
+        for (int64_t i = 0; i < 2 * ctx->n; ++i) host[i] = double(f[i]);
+    }
+    QND_API_END
+}
+
+int qnd_synchronize(qnd_ctx* ctx) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    set_device(ctx);
+    QND_CK(cudaStreamSynchronize(ctx->stream));
+    QND_CK(cudaGetLastError());
+    QND_API_END
+}
+
+int qnd_step_imag(qnd_ctx* ctx, void* psi_dev, int64_t nsteps) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_dev);
+    set_device(ctx);
+    imag_steps(ctx, psi_dev, nsteps, nullptr);
+    QND_CK(cudaGetLastError());
+    QND_API_END
+}
+
+int qnd_to_p(qnd_ctx* ctx, void* psi_dev) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_dev);
+    set_device(ctx);
+    unitary_fft(ctx, psi_dev, true);
+    QND_API_END
+}
+
+int qnd_to_r(qnd_ctx* ctx, void* psi_dev) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_dev);
+    set_device(ctx);
+    unitary_fft(ctx, psi_dev, false);
+    QND_API_END
+}
+
+int qnd_step_length(qnd_ctx* ctx, void* psi_p_dev, const double* E_host, int64_t nsteps) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_p_dev);
+    if (nsteps <= 0) return QND_OK;
+    QND_NEED(E_host);
+    set_device(ctx);
+    unitary_fft(ctx, psi_p_dev, false);
+    for (int64_t c0 = 0; c0 < nsteps; c0 += CHUNK) {
+        const int64_t ch = std::min(CHUNK, nsteps - c0);
+        upload_field_chunk(ctx, E_host + size_t(c0) * ctx->s * ctx->dim, ch, false);
+        for (int64_t k = 0; k < ch; ++k) length_step(ctx, psi_p_dev, k, {}, false);
+    }
+    unitary_fft(ctx, psi_p_dev, true);
+    QND_CK(cudaGetLastError());
+    QND_API_END
+}
+
+int qnd_step_velocity(qnd_ctx* ctx, void* psi_dev, const double* A_host, int64_t nsteps) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_dev);
+    if (nsteps <= 0) return QND_OK;
+    QND_NEED(A_host);
+    set_device(ctx);
+    for (int64_t c0 = 0; c0 < nsteps; c0 += CHUNK) {
+        const int64_t ch = std::min(CHUNK, nsteps - c0);
+        upload_field_chunk(ctx, A_host + size_t(c0) * ctx->s * ctx->dim, ch, true);
+        for (int64_t k = 0; k < ch; ++k) velocity_step(ctx, psi_dev, k, {}, false);
+    }
+    QND_CK(cudaGetLastError());
+    QND_API_END
+}
+
+int qnd_run_length(qnd_ctx* ctx, void* psi_r_dev, const double* E_host, int64_t nsteps, int nobs,
+                   const char* const* names, double* obs_host) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_r_dev);
+    if (nsteps <= 0) return QND_OK;
+    QND_NEED(E_host);
+    if (nobs > 0) QND_NEED(names);
+    set_device(ctx);
+    int nv = 0;
+    parse_obs(ctx, nobs, names, &nv);
+    if (nv > 0) QND_NEED(obs_host);
+    run_realtime(ctx, psi_r_dev, E_host, nullptr, nsteps, nobs, names, obs_host, false);
+    QND_API_END
+}
+
+int qnd_run_velocity(qnd_ctx* ctx, void* psi_r_dev, const double* A_host, const double* alpha_host, int64_t nsteps,
+                     int nobs, const char* const* names, double* obs_host) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_r_dev);
+    if (nsteps <= 0) return QND_OK;
+    QND_NEED(A_host);
+    if (nobs > 0) QND_NEED(names);
+    set_device(ctx);
+    int nv = 0;
+    parse_obs(ctx, nobs, names, &nv);
+    if (nv > 0) {
+        QND_NEED(obs_host);
+        QND_NEED(alpha_host);
+    }
+    run_realtime(ctx, psi_r_dev, A_host, alpha_host, nsteps, nobs, names, obs_host, true);
+    QND_API_END
+}
+
+int qnd_gram_schmidt(qnd_ctx* ctx, void* const* states_dev, int j, double* norm2_out) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(states_dev);
+    if (j < 0) QND_FAIL(QND_EINVAL, "state index %d < 0", j);
+    for (int k = 0; k <= j; ++k) QND_NEED(states_dev[k]);
+    set_device(ctx);
+    gs_project(ctx, states_dev, j);
+    if (norm2_out) {
+        QND_CK(cudaMemcpyAsync(norm2_out, ctx->scal.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    check_gs_flag(ctx, j);
+    scale_state(ctx, states_dev[j], ctx->scal.as<double>() + 1);
+    QND_CK(cudaStreamSynchronize(ctx->stream));
+    QND_API_END
+}
+
+int qnd_imag_propagate(qnd_ctx* ctx, void* const* states_dev, int j, int64_t nsteps) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(states_dev);
+    if (j < 0) QND_FAIL(QND_EINVAL, "state index %d < 0", j);
+    for (int k = 0; k <= j; ++k) QND_NEED(states_dev[k]);
+    if (nsteps <= 0) return QND_OK;
+    set_device(ctx);
+    const double* pending = nullptr;
+    for (int64_t st = 0; st < nsteps; ++st) {
+        imag_steps(ctx, states_dev[j], 1, pending);
+        gs_project(ctx, states_dev, j);
+        pending = ctx->scal.as<double>() + 1;
+        if ((st & 255) == 255) check_gs_flag(ctx, j);
+    }
+    scale_state(ctx, states_dev[j], pending);
+    check_gs_flag(ctx, j);
+    QND_API_END
+}
+
+int qnd_run_length_dev(qnd_ctx* ctx, void* psi_r_dev, const double* E_dev, int64_t nsteps, int nobs,
+                       const char* const* names, double* obs_dev) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_r_dev);
+    if (nsteps <= 0) return QND_OK;
+    QND_NEED(E_dev);
+    if (nobs > 0) QND_NEED(names);
+    set_device(ctx);
+    int nv = 0;
+    auto items = parse_obs(ctx, nobs, names, &nv);
+    if (nv > 0) QND_NEED(obs_dev);
+    const bool fused = all_rspace(items);
+    const bool masked = has_mask(ctx);
+    const double zero[MAX_DIM] = {0, 0, 0};
+    for (int64_t c0 = 0; c0 < nsteps; c0 += CHUNK) {
+        const int64_t ch = std::min(CHUNK, nsteps - c0);
+        build_field_tables(ctx, E_dev + size_t(c0) * ctx->s * ctx->dim, ch, false);
+        for (int64_t k = 0; k < ch; ++k) {
+            double* row = nv > 0 ? obs_dev + size_t(c0 + k) * nv : nullptr;
+            std::vector<RedDesc> fin;
+            if (nv > 0 && fused) fin = rspace_red(ctx, items, row);
+            length_step(ctx, psi_r_dev, k, fin, masked);
+            if (nv > 0 && !fused) eval_obs(ctx, psi_r_dev, items, zero, row);
+        }
+    }
+    QND_CK(cudaGetLastError());
+    QND_API_END
+}
+
+int qnd_ctx_set_profiling(qnd_ctx* ctx, int enable) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    ctx->profiling = enable != 0;
+    QND_API_END
+}
+
+int qnd_ctx_get_profile(qnd_ctx* ctx, int64_t* kernels_launched, int64_t* passes_timed, double* pass_ms_total,
+                        int reset) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    set_device(ctx);
+    QND_CK(cudaStreamSynchronize(ctx->stream));
+    double total = 0;
+    for (auto& pr : ctx->prof_pairs) {
+        float ms = 0;
+        QND_CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        total += ms;
+    }
+    if (kernels_launched) *kernels_launched = ctx->kernels_launched;
+    if (passes_timed) *passes_timed = int64_t(ctx->prof_pairs.size());
+    if (pass_ms_total) *pass_ms_total = total;
+    if (reset) {
+        for (auto& pr : ctx->prof_pairs) {
+            ctx->event_pool.push_back(pr.first);
+            ctx->event_pool.push_back(pr.second);
+        }
+        ctx->prof_pairs.clear();
+        ctx->kernels_launched = 0;
+    }
+    QND_API_END
+}
+
+int qnd_observable_count(qnd_ctx* ctx, int nobs, const char* const* names, int* nvalues) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(nvalues);
+    if (nobs > 0) QND_NEED(names);
+    int nv = 0;
+    for (int k = 0; k < nobs; ++k) {
+        const char* nm = names[k] ? names[k] : "";
+        if (!strcmp(nm, "norm") || !strcmp(nm, "energy") || !strcmp(nm, "Lz")) nv += 1;
+        else if (!strcmp(nm, "dipole_r") || !strcmp(nm, "dipole_v") || !strcmp(nm, "accel")) nv += ctx->dim;
+    }
+    *nvalues = nv;
+    QND_API_END
+}
+
+int qnd_observables(qnd_ctx* ctx, const void* psi_r_dev, int nobs, const char* const* names, const double* alpha,
+                    double* out_host) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_r_dev);
+    if (nobs > 0) QND_NEED(names);
+    set_device(ctx);
+    int nv = 0;
+    auto items = parse_obs(ctx, nobs, names, &nv);
+    if (nv == 0) return QND_OK;
+    QND_NEED(out_host);
+    double zero[MAX_DIM] = {0, 0, 0};
+    ctx->obs_dev.ensure(size_t(nv) * sizeof(double) * 2);
+    eval_obs(ctx, psi_r_dev, items, alpha ? alpha : zero, ctx->obs_dev.as<double>());
+    QND_CK(cudaMemcpyAsync(out_host, ctx->obs_dev.p, nv * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    QND_CK(cudaStreamSynchronize(ctx->stream));
+    QND_API_END
+}
+
+int qnd_energies(qnd_ctx* ctx, const void* psi_r_dev, int n, double* out_host) {
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_r_dev);
+    if (n <= 0) return QND_OK;
+    QND_NEED(out_host);
+    set_device(ctx);
+    ctx->obs_dev.ensure(size_t(n) * sizeof(double) * 2);
+    energy_moments(ctx, psi_r_dev, n, ctx->obs_dev.as<double>());
+    QND_CK(cudaMemcpyAsync(out_host, ctx->obs_dev.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    QND_CK(cudaStreamSynchronize(ctx->stream));
+    QND_API_END
+}
+
+}  // extern "C"

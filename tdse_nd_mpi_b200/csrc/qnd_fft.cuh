@@ -1,0 +1,218 @@
+// qnd_fft.cuh — in-CTA power-of-two FFT building blocks for sm_100a.
+//
+// A line of L complex values is spread over T = L/E threads, E values per
+// thread in registers. The transform is a Stockham autosort FFT (the
+// formulation of Govindaraju et al., "High Performance Discrete Fourier
+// Transforms on Graphics Processors", SC'08): stage k with radix R and span Ns
+// reads x[j + r*L/R], twiddles by W_{Ns*R}^{(j mod Ns)*r}, does an R-point DFT in
+// registers and writes to (j/Ns)*Ns*R + (j mod Ns) + r*Ns. Between stages data is
+// exchanged through shared memory with a padded layout (one 16-element pad per
+// 16 values) that keeps the exchanges free of bank conflicts.
+//
+// Two facts make the fused passes cheap:
+//  * the first stage reads x[tid + r*T] and the last stage writes
+//    x[tid + r*T]: global loads/stores are coalesced straight to/from registers;
+//  * the last forward stage and the first inverse stage hold the same elements
+//    in the same registers, so a spectral multiply between them needs no
+//    shared-memory round trip.
+//
+// Sign convention is FFTW's: forward exp(-2*pi*i*k*n/L), inverse exp(+...), both
+// unnormalised (the reference's plans, meshgrid.c:166-167).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <utility>
+
+namespace qnd {
+
+template <typename R> struct cvec;
+template <> struct cvec<double> { using T = double2; };
+template <> struct cvec<float> { using T = float2; };
+template <typename R> using cplx_t = typename cvec<R>::T;
+
+template <typename V> __device__ __forceinline__ V cadd(V a, V b) { return V{a.x + b.x, a.y + b.y}; }
+template <typename V> __device__ __forceinline__ V csub(V a, V b) { return V{a.x - b.x, a.y - b.y}; }
+template <typename V> __device__ __forceinline__ V cmul(V a, V b) {
+    return V{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+// a * conj(b)
+template <typename V> __device__ __forceinline__ V cmulc(V a, V b) {
+    return V{a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y};
+}
+template <typename V, typename S> __device__ __forceinline__ V cscale(V a, S s) { return V{a.x * s, a.y * s}; }
+
+__host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
+
+// Correctly rounded cos/sin of pi/4 and pi/8 (exact mathematical constants).
+#define QND_R2 0.7071067811865476
+#define QND_C8 0.9238795325112867
+#define QND_S8 0.3826834323650898
+
+// Multiply a by exp(SIGN * 2*pi*i*K/N) for N <= 16, with the trivial angles special-cased.
+template <int N, int K, int SIGN, typename V> __device__ __forceinline__ V twiddle_const(V a) {
+    using S = decltype(a.x);
+    constexpr int k = ((K % N) + N) % N;
+    constexpr int e = k * (16 / N);  // angle in units of 2*pi/16
+    static_assert(16 % N == 0, "twiddle_const handles N <= 16");
+    if constexpr (e == 0) {
+        return a;
+    } else if constexpr (e == 8) {
+        return V{-a.x, -a.y};
+    } else if constexpr (e == 4 || e == 12) {
+        // exp(+-i*pi/2) = +-i ; (x+iy)*i = -y+ix
+        constexpr int s = (e == 4 ? 1 : -1) * SIGN;
+        if constexpr (s > 0) return V{-a.y, a.x};
+        else return V{a.y, -a.x};
+    } else {
+        // general angle: cos/sin from the pi/8 table with exact symmetry
+        constexpr int q = e % 4;  // 1,2,3 within the quadrant
+        constexpr int quad = e / 4;
+        constexpr double c0 = q == 1 ? QND_C8 : (q == 2 ? QND_R2 : QND_S8);
+        constexpr double s0 = q == 1 ? QND_S8 : (q == 2 ? QND_R2 : QND_C8);
+        // rotate (c0, s0) by quad * pi/2
+        constexpr double c = quad == 0 ? c0 : (quad == 1 ? -s0 : (quad == 2 ? -c0 : s0));
+        constexpr double sn = quad == 0 ? s0 : (quad == 1 ? c0 : (quad == 2 ? -s0 : -c0));
+        const S cw = S(c), sw = S(SIGN * sn);
+        return V{a.x * cw - a.y * sw, a.x * sw + a.y * cw};
+    }
+}
+
+// In-register R-point DFT (natural order in and out), radix-2 decimation in time.
+template <int R, int SIGN> struct RegDFT {
+    template <typename V, int... K>
+    __device__ __forceinline__ static void combine(V* v, const V* e, const V* o, std::integer_sequence<int, K...>) {
+        ((void)([&] {
+             V t = twiddle_const<R, K, SIGN>(o[K]);
+             v[K] = cadd(e[K], t);
+             v[K + R / 2] = csub(e[K], t);
+         }()),
+         ...);
+    }
+    template <typename V> __device__ __forceinline__ static void run(V* v) {
+        V e[R / 2], o[R / 2];
+#pragma unroll
+        for (int i = 0; i < R / 2; ++i) {
+            e[i] = v[2 * i];
+            o[i] = v[2 * i + 1];
+        }
+        RegDFT<R / 2, SIGN>::run(e);
+        RegDFT<R / 2, SIGN>::run(o);
+        combine(v, e, o, std::make_integer_sequence<int, R / 2>{});
+    }
+};
+template <int SIGN> struct RegDFT<1, SIGN> {
+    template <typename V> __device__ __forceinline__ static void run(V*) {}
+};
+template <int SIGN> struct RegDFT<2, SIGN> {
+    template <typename V> __device__ __forceinline__ static void run(V* v) {
+        V a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    }
+};
+
+// Shared-memory index with one pad slot per 16 values.
+__device__ __forceinline__ int spad(int i) { return i + (i >> 4); }
+
+// Compile-time description of the stage sequence for a length-L line with E values per thread.
+template <int L, int E> struct FFTPlan {
+    static constexpr int T = L / E;                        // threads per line
+    static constexpr int LOGL = ilog2(L);
+    static constexpr int LOGE = ilog2(E);
+    static constexpr int NSTAGE = (LOGL + LOGE - 1) / LOGE; // ceil(LOGL / LOGE)
+    __host__ __device__ static constexpr int radix(int st) {
+        return st < NSTAGE - 1 ? E : (1 << (LOGL - LOGE * (NSTAGE - 1)));
+    }
+    __host__ __device__ static constexpr int span(int st) { return st == 0 ? 1 : span(st - 1) * radix(st - 1); }
+    // Offset of stage st's twiddles in the per-plan table ([j mod Ns][r-1] layout).
+    __host__ __device__ static constexpr int tw_offset(int st) {
+        return st <= 1 ? 0 : tw_offset(st - 1) + span(st - 1) * (radix(st - 1) - 1);
+    }
+    __host__ __device__ static constexpr int tw_size() { return tw_offset(NSTAGE) ; }
+    static constexpr int SMEM_LINE = L >= 16 ? L + L / 16 : L;  // padded values per line (before line padding)
+};
+
+// One Stockham stage on the thread's E registers (B = E/R butterflies, j = tid + b*T).
+// Input registers hold x[j + r*L/R] for butterfly b at v[b*R + r]; output registers hold
+// the butterfly outputs in the same slots. Twiddles come from smem table tw (forward sign).
+template <int L, int E, int ST, int SIGN, typename V>
+__device__ __forceinline__ void fft_stage_regs(V* v, int tid, const V* __restrict__ tw) {
+    using P = FFTPlan<L, E>;
+    constexpr int R = P::radix(ST);
+    constexpr int Ns = P::span(ST);
+    constexpr int B = E / R;
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+        V* u = v + b * R;
+        if constexpr (Ns > 1) {
+            const int j = tid + b * P::T;
+            const int jm = j & (Ns - 1);
+            const V* t = tw + P::tw_offset(ST) + jm * (R - 1);
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                V w = t[r - 1];
+                if constexpr (SIGN > 0) w.y = -w.y;
+                u[r] = cmul(u[r], w);
+            }
+        }
+        RegDFT<R, SIGN>::run(u);
+    }
+}
+
+// Register slot of element index (tid + u*T) held after the LAST stage (position j + r*Ns_last,
+// j = tid + b*T): u = b + r*B_last. Loading order before the FIRST stage is slot b*R0 + r for
+// element j + r*L/R0 with j = tid + b*T, i.e. u = b + r*B_0. For the first stage R0 = E, B_0 = 1.
+template <int L, int E> struct SlotMap {
+    using P = FFTPlan<L, E>;
+    static constexpr int RL = P::radix(P::NSTAGE - 1);
+    static constexpr int BL = E / RL;
+    // slot holding element tid + u*T after the last stage
+    __host__ __device__ static constexpr int last_slot(int u) { return (u % BL) * RL + (u / BL); }
+};
+
+// Full FFT of one line held in registers: on entry v[u] = x[tid + u*T], on exit
+// v[u] = X[tid + u*T] (both in natural slots). `line` is this line's padded smem
+// buffer; `sync` is the CTA barrier (all lines of a CTA transform in lockstep).
+// Call as fft_line_stages<L, E, SIGN, 0>(...).
+template <int L, int E, int SIGN, int ST, typename V, typename Sync>
+__device__ __forceinline__ void fft_line_stages(V* v, int tid, V* line, const V* __restrict__ tw, Sync sync) {
+    using P = FFTPlan<L, E>;
+    constexpr int T = P::T;
+    constexpr int R = P::radix(ST);
+    constexpr int Ns = P::span(ST);
+    constexpr int B = E / R;
+    fft_stage_regs<L, E, ST, SIGN>(v, tid, tw);
+    if constexpr (ST + 1 < P::NSTAGE) {
+        // exchange: store outputs of stage ST, load inputs of stage ST+1
+        constexpr int R2 = P::radix(ST + 1);
+        constexpr int B2 = E / R2;
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const int j = tid + b * T;
+            const int base = (j / Ns) * Ns * R + (j & (Ns - 1));
+#pragma unroll
+            for (int r = 0; r < R; ++r) line[spad(base + r * Ns)] = v[b * R + r];
+        }
+        sync();
+#pragma unroll
+        for (int b = 0; b < B2; ++b) {
+            const int j = tid + b * T;
+#pragma unroll
+            for (int r = 0; r < R2; ++r) v[b * R2 + r] = line[spad(j + r * (L / R2))];
+        }
+        sync();
+        fft_line_stages<L, E, SIGN, ST + 1>(v, tid, line, tw, sync);
+    } else {
+        // last stage: outputs at positions j + r*Ns (j = tid + b*T < Ns); reorder registers to
+        // natural slots v[u] = X[tid + u*T].
+        V tmp[E];
+#pragma unroll
+        for (int u = 0; u < E; ++u) tmp[u] = v[SlotMap<L, E>::last_slot(u)];
+#pragma unroll
+        for (int u = 0; u < E; ++u) v[u] = tmp[u];
+    }
+}
+
+}  // namespace qnd

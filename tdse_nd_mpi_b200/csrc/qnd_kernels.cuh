@@ -1,0 +1,80 @@
+// qnd_kernels.cuh — kernel registry and auxiliary kernels shared by the engine.
+#pragma once
+
+#include "qnd_pass.cuh"
+
+namespace qnd {
+
+struct PassKernelInfo {
+    const void* fn;
+    int nt;       // threads per CTA
+    size_t smem;  // dynamic shared memory bytes
+    int G;        // lines per CTA
+    int tw_size;  // twiddle entries expected in the plan table
+};
+
+// Defined once per line length in qnd_pass_inst.cu (compiled with -DQND_L=...).
+template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int mode);
+
+// Host-side copy of the FFTPlan stage structure for a runtime line length.
+struct HostPlan {
+    int L, E, T, nstage;
+    int radix[16], span[16];
+    int tw_size;
+    explicit HostPlan(int L_) : L(L_) {
+        E = L < 16 ? L : 16;
+        T = L / E;
+        int logl = 0, loge = 0;
+        while ((1 << logl) < L) ++logl;
+        while ((1 << loge) < E) ++loge;
+        nstage = loge ? (logl + loge - 1) / loge : 1;
+        int ns = 1;
+        tw_size = 0;
+        for (int st = 0; st < nstage; ++st) {
+            radix[st] = st < nstage - 1 ? E : (1 << (logl - loge * (nstage - 1)));
+            span[st] = ns;
+            if (st >= 1) tw_size += ns * (radix[st] - 1);
+            ns *= radix[st];
+        }
+    }
+};
+
+constexpr int GS_MAXK = 32;  // states a Gram-Schmidt call can orthogonalise against
+
+template <typename R> struct GSArgs {
+    using V = cplx_t<R>;
+    V* psi;                   // state being orthonormalised
+    const V* states[GS_MAXK]; // previous states
+    int k0, nk;               // dot kernel: states[k0 .. k0+nk) (nk <= MAX_RED/2)
+    int j;                    // axpy kernel: subtract states[0..j)
+    const double* coef;       // [2*j] (re, im) projection coefficients
+    long long n;
+    RedDesc red;
+};
+
+template <typename R> void launch_gs_dot(const GSArgs<R>& a, cudaStream_t st, int nblocks);
+template <typename R> void launch_gs_axpy(const GSArgs<R>& a, cudaStream_t st, int nblocks);
+template <typename R> void launch_grid_reduce(const PassArgs<R>& a, long long n, cudaStream_t st, int nblocks);
+template <typename R> void launch_scale(cplx_t<R>* psi, long long n, const double* scale_dev, cudaStream_t st);
+void launch_gs_finalize(const double* norm2, double tol, double* scale, int* flag, cudaStream_t st);
+
+// Per-step field tables for a chunk of steps; each (step, stage) block holds sum_j N_j values,
+// axis j at offset off[j].
+//  length:   out = exp(-i h_ia r_j[i] E[step][ia][j])                     (r-space, per axis)
+//  velocity: out = exp(-i h_ia (p_j^2/2 + (p_j + A_j/2) A_j)) / N_j        (k-space, per axis)
+struct FieldTableArgs {
+    const double* field;  // [nsteps][s][dim]
+    const double* axes;   // concatenated r (length) or p (velocity) axes
+    int nsteps, s, dim;
+    int nr[MAX_DIM], off[MAX_DIM], ntot;
+    double h[32];
+    int velocity;
+};
+template <typename R> void launch_field_tables(const FieldTableArgs& a, cplx_t<R>* out, cudaStream_t st);
+
+// Per-axis tables that depend on a runtime shift alpha:
+//   mode 0: w[k] = p[k] + alpha (double)            dipole_v weights
+//   mode 1: spec[k] = (p[k] + alpha) / N (complex)   Lz operator
+template <typename R> void launch_axis_table(int mode, const double* p, int N, double alpha, void* out, cudaStream_t st);
+
+}  // namespace qnd

@@ -1,0 +1,31 @@
+// qnd_pass_inst.cu — instantiates the fused axis-pass kernels for one line length.
+// The build compiles this file once per supported length with -DQND_L=<L>.
+#include "qnd_kernels.cuh"
+
+#ifndef QND_L
+#error "compile with -DQND_L=<line length>"
+#endif
+
+namespace qnd {
+
+template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int mode) {
+    using SH = PassShape<R, L>;
+    const void* fn = nullptr;
+#define QND_PICK(M) \
+    (strided ? (const void*)&qnd_pass_kernel<R, L, true, M> : (const void*)&qnd_pass_kernel<R, L, false, M>)
+    switch (mode) {
+    case PM_SANDWICH: fn = QND_PICK(PM_SANDWICH); break;
+    case PM_FFT_FWD: fn = QND_PICK(PM_FFT_FWD); break;
+    case PM_FFT_INV: fn = QND_PICK(PM_FFT_INV); break;
+    case PM_SPECRED: fn = QND_PICK(PM_SPECRED); break;
+    case PM_APPLY: fn = QND_PICK(PM_APPLY); break;
+    default: fn = nullptr;
+    }
+#undef QND_PICK
+    return PassKernelInfo{fn, SH::NT, SH::SMEM, SH::G, FFTPlan<L, SH::E>::tw_size()};
+}
+
+template PassKernelInfo pass_kernel_info<double, QND_L>(bool, int);
+template PassKernelInfo pass_kernel_info<float, QND_L>(bool, int);
+
+}  // namespace qnd
