@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -146,6 +147,8 @@ struct qnd_ctx {
     DevBuf scratch_a, scratch_b;
     std::vector<char> host_tmp;
 
+    int num_sms = 148;
+    bool pdl = true;  // programmatic dependent launch between passes
     bool profiling = false;
     int64_t kernels_launched = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pairs;
@@ -162,7 +165,7 @@ namespace qnd {
 // Twiddles of HostPlan(L) in the [j mod Ns][r-1] layout, exp(-2 pi i jm r / (Ns R)), in long double.
 static void build_twiddles(qnd_ctx* c, int ax) {
     const int L = int(c->nr[ax]);
-    HostPlan pl(L);
+    HostPlan pl(L, lookup_pass(c->fp64, L, false, PM_SANDWICH).E);
     std::vector<double> tw(2 * size_t(pl.tw_size > 0 ? pl.tw_size : 1));
     const long double two_pi = 6.283185307179586476925286766559005768L;
     size_t o = 0;
@@ -179,11 +182,11 @@ static void build_twiddles(qnd_ctx* c, int ax) {
     const size_t cnt = size_t(pl.tw_size > 0 ? pl.tw_size : 1);
     c->tw[ax].ensure(cnt * c->elem());
     if (c->fp64) {
-        QND_CK(cudaMemcpy(c->tw[ax].p, tw.data(), cnt * 16, cudaMemcpyHostToDevice));
+        QND_CK(cudaMemcpyAsync(c->tw[ax].p, tw.data(), cnt * 16, cudaMemcpyHostToDevice, c->stream));
     } else {
         std::vector<float> f(2 * cnt);
         for (size_t i = 0; i < 2 * cnt; ++i) f[i] = float(tw[i]);
-        QND_CK(cudaMemcpy(c->tw[ax].p, f.data(), cnt * 8, cudaMemcpyHostToDevice));
+        QND_CK(cudaMemcpyAsync(c->tw[ax].p, f.data(), cnt * 8, cudaMemcpyHostToDevice, c->stream));
     }
 }
 
@@ -192,7 +195,7 @@ static void upload_cplx(qnd_ctx* c, DevBuf& dst, const std::vector<double>& v) {
     const size_t n = v.size() / 2;
     dst.ensure(n * c->elem());
     if (c->fp64) {
-        QND_CK(cudaMemcpy(dst.p, v.data(), n * 16, cudaMemcpyHostToDevice));
+        QND_CK(cudaMemcpyAsync(dst.p, v.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
     } else {
         std::vector<float> f(2 * n);
         for (size_t i = 0; i < 2 * n; ++i) {
@@ -200,7 +203,7 @@ static void upload_cplx(qnd_ctx* c, DevBuf& dst, const std::vector<double>& v) {
             if (std::isinf(f[i]) && !std::isinf(v[i]))
                 QND_FAIL(QND_EUNSUPPORTED, "a phase/decay factor exceeds the FP32 range: use QND_FP64 for this case");
         }
-        QND_CK(cudaMemcpy(dst.p, f.data(), n * 8, cudaMemcpyHostToDevice));
+        QND_CK(cudaMemcpyAsync(dst.p, f.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
     }
 }
 
@@ -208,7 +211,7 @@ static void upload_real(qnd_ctx* c, DevBuf& dst, const std::vector<double>& v) {
     const size_t n = v.size();
     dst.ensure(n * c->rsize());
     if (c->fp64) {
-        QND_CK(cudaMemcpy(dst.p, v.data(), n * 8, cudaMemcpyHostToDevice));
+        QND_CK(cudaMemcpyAsync(dst.p, v.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
     } else {
         std::vector<float> f(n);
         for (size_t i = 0; i < n; ++i) {
@@ -216,13 +219,15 @@ static void upload_real(qnd_ctx* c, DevBuf& dst, const std::vector<double>& v) {
             if (std::isinf(f[i]) && !std::isinf(v[i]))
                 QND_FAIL(QND_EUNSUPPORTED, "a decay factor exceeds the FP32 range: use QND_FP64 for this case");
         }
-        QND_CK(cudaMemcpy(dst.p, f.data(), n * 4, cudaMemcpyHostToDevice));
+        QND_CK(cudaMemcpyAsync(dst.p, f.data(), n * 4, cudaMemcpyHostToDevice, c->stream));
     }
 }
 
-static void upload_f64(DevBuf& dst, const std::vector<double>& v) {
+// Every upload is ordered on the context's stream: a synchronous cudaMemcpy from pageable memory may
+// return before its DMA lands, and the kernels that read the table run on the context's stream.
+static void upload_f64(qnd_ctx* c, DevBuf& dst, const std::vector<double>& v) {
     dst.ensure(v.size() * 8);
-    QND_CK(cudaMemcpy(dst.p, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+    QND_CK(cudaMemcpyAsync(dst.p, v.data(), v.size() * 8, cudaMemcpyHostToDevice, c->stream));
 }
 
 enum SpecKind { SP_LENGTH = 0, SP_IMAG = 1, SP_KIN = 2 };
@@ -338,6 +343,7 @@ struct PassSpec {
     const void* epi_cplx = nullptr;
     const void* ax_cplx[MAX_DIM] = {nullptr, nullptr, nullptr};
     const void* ax_real[MAX_DIM] = {nullptr, nullptr, nullptr};
+    int ax_in_prologue = 0;
     double scale = 1.0;
     int apply_acc = 0;
     const double* apply_vtab = nullptr;
@@ -349,7 +355,7 @@ static void ensure_red_scratch(qnd_ctx* c, long long blocks) {
     if (c->partials.bytes < need) c->partials.ensure(need);
     if (!c->counter.p) {
         c->counter.ensure(64);
-        QND_CK(cudaMemset(c->counter.p, 0, 64));
+        QND_CK(cudaMemsetAsync(c->counter.p, 0, 64, c->stream));
     }
 }
 
@@ -358,6 +364,7 @@ template <typename R> static void fill_args(qnd_ctx* c, const PassSpec& ps, Pass
     std::memset(&a, 0, sizeof a);
     a.psi = static_cast<V*>(ps.psi);
     a.dst = static_cast<V*>(ps.dst);
+    a.axis = ps.axis;
     a.partner = static_cast<const V*>(ps.partner);
     a.dim = c->dim;
     for (int k = 0; k < MAX_DIM; ++k) {
@@ -374,12 +381,19 @@ template <typename R> static void fill_args(qnd_ctx* c, const PassSpec& ps, Pass
         a.ax_cplx[k] = static_cast<const V*>(ps.ax_cplx[k]);
         a.ax_real[k] = static_cast<const R*>(ps.ax_real[k]);
     }
+    a.ax_in_prologue = ps.ax_in_prologue;
     a.scale = R(ps.scale);
     a.apply_acc = ps.apply_acc;
     a.apply_vtab = ps.apply_vtab;
     a.red = ps.red;
 }
 
+struct LaunchCfg {
+    int blocks_per_sm = 0;
+};
+
+// Launch one fused axis pass: persistent grid (at most the resident CTAs), programmatic
+// dependent launch so the pass's prologue overlaps the tail of the previous kernel.
 static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     const int ax = ps.axis;
     const int L = int(c->nr[ax]);
@@ -387,18 +401,23 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     const bool strided = log2S > 0;
     const PassKernelInfo info = lookup_pass(c->fp64, L, strided, ps.mode);
     const long long nlines = c->n / L;
-    const long long blocks = (nlines + info.G - 1) / info.G;
+    const long long ngroups = (nlines + info.G - 1) / info.G;
+    static std::map<std::pair<const void*, int>, LaunchCfg> configured;  // per (kernel, device)
+    auto cfg_key = std::make_pair(info.fn, c->device);
+    auto cfg_it = configured.find(cfg_key);
+    if (cfg_it == configured.end()) {
+        QND_CK(cudaFuncSetAttribute(info.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(info.smem)));
+        LaunchCfg cfg;
+        QND_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cfg.blocks_per_sm, info.fn, info.nt, info.smem));
+        if (cfg.blocks_per_sm < 1) QND_FAIL(QND_ECUDA, "pass kernel for L=%d does not fit on an SM", L);
+        cfg_it = configured.emplace(cfg_key, cfg).first;
+    }
+    const long long blocks = std::max<long long>(1, ngroups);
     RedDesc red = ps.red;
     if (red.n) {
         ensure_red_scratch(c, blocks);
         red.partials = c->partials.as<double>();
         red.counter = c->counter.as<unsigned int>();
-    }
-    static std::map<std::pair<const void*, int>, bool> configured;  // per (kernel, device)
-    auto cfg_key = std::make_pair(info.fn, c->device);
-    if (!configured[cfg_key]) {
-        QND_CK(cudaFuncSetAttribute(info.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(info.smem)));
-        configured[cfg_key] = true;
     }
     std::pair<cudaEvent_t, cudaEvent_t> ev{nullptr, nullptr};
     if (c->profiling) {
@@ -412,6 +431,16 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         }
         QND_CK(cudaEventRecord(ev.first, c->stream));
     }
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(unsigned(blocks));
+    lc.blockDim = dim3(unsigned(info.nt));
+    lc.dynamicSmemBytes = info.smem;
+    lc.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = c->pdl ? 1 : 0;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
     if (c->fp64) {
         PassArgs<double> a;
         fill_args<double>(c, ps, a);
@@ -420,7 +449,7 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         a.log2S = log2S;
         a.nlines = nlines;
         void* args[] = {&a};
-        QND_CK(cudaLaunchKernel(info.fn, dim3(unsigned(blocks)), dim3(info.nt), args, info.smem, c->stream));
+        QND_CK(cudaLaunchKernelExC(&lc, info.fn, args));
     } else {
         PassArgs<float> a;
         fill_args<float>(c, ps, a);
@@ -429,7 +458,7 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         a.log2S = log2S;
         a.nlines = nlines;
         void* args[] = {&a};
-        QND_CK(cudaLaunchKernel(info.fn, dim3(unsigned(blocks)), dim3(info.nt), args, info.smem, c->stream));
+        QND_CK(cudaLaunchKernelExC(&lc, info.fn, args));
     }
     c->kernels_launched++;
     if (c->profiling) {
@@ -543,7 +572,7 @@ static void ensure_scratch_state(qnd_ctx* c, DevBuf& b) { b.ensure(size_t(c->n) 
 
 static void ensure_vpot_dev(qnd_ctx* c) {
     if (c->vpot.empty()) QND_FAIL(QND_EINVAL, "no potential set");
-    if (!c->vpot_dev.p) upload_f64(c->vpot_dev, c->vpot);
+    if (!c->vpot_dev.p) upload_f64(c, c->vpot_dev, c->vpot);
 }
 
 // out[m-1] = Re <psi | H^m | psi> dNr for m = 1..nmom (calculate_observables.c:146-175), written to dev.
@@ -673,18 +702,19 @@ static void imag_steps(qnd_ctx* c, void* psi, int64_t nsteps, const double* pro_
     auto order = pass_order(c);
     for (int64_t st = 0; st < nsteps; ++st) {
         for (int ia = 0; ia < c->s; ++ia) {
-            const double a = c->as[2 * ia], b = c->as[2 * ia + 1], h = a + b;
+            const double h = c->as[2 * ia] + c->as[2 * ia + 1];
             for (size_t q = 0; q < order.size(); ++q) {
                 PassSpec ps;
                 ps.axis = order[q];
                 ps.psi = psi;
                 ps.spec = spec_table(c, SP_IMAG, order[q], h);
-                if (q == 0 && ia == 0) {
-                    ps.pro_real = rtab(c, RT_IMAG, a, NO_COEF);
-                    if (st == 0) ps.pro_scale = pro_scale;
+                if (q == 0) {
+                    // factors before K(h_ia): V(a_0) at the start, V(a_{2ia-1}) V(a_{2ia}) in between
+                    ps.pro_real = ia == 0 ? rtab(c, RT_IMAG, c->as[0], NO_COEF)
+                                          : rtab(c, RT_IMAG, c->as[2 * ia - 1], c->as[2 * ia]);
+                    if (ia == 0 && st == 0) ps.pro_scale = pro_scale;
                 }
-                if (q + 1 == order.size())
-                    ps.epi_real = ia + 1 < c->s ? rtab(c, RT_IMAG, b, c->as[2 * ia + 2]) : rtab(c, RT_IMAG, b, NO_COEF);
+                if (q + 1 == order.size() && ia + 1 == c->s) ps.epi_real = rtab(c, RT_IMAG, c->as[2 * c->s - 1], NO_COEF);
                 launch_pass(c, ps);
             }
         }
@@ -733,7 +763,10 @@ static bool has_mask(const qnd_ctx* c) {
 }
 
 // One length-gauge step in r-space (chunk-local step index lst for the field tables).
-// fin: reductions fused into the final pass (may have n == 0); masked: apply the step mask.
+// fin: reductions fused into the final pass (may be empty); masked: apply the step mask.
+// Each kinetic sandwich runs the contiguous axis first; the potential/laser factor V(h) that
+// separates two sandwiches is applied as the prologue of the next sandwich's first pass, where
+// its full-grid table is read with coalesced accesses alongside the state.
 static void length_step(qnd_ctx* c, void* psi, int64_t lst, const std::vector<RedDesc>& fin, bool masked) {
     auto order = pass_order(c);
     for (int ia = 0; ia <= c->s; ++ia) {
@@ -747,16 +780,16 @@ static void length_step(qnd_ctx* c, void* psi, int64_t lst, const std::vector<Re
             ps.axis = order[q];
             ps.psi = psi;
             ps.spec = spec_table(c, SP_LENGTH, order[q], kc);
-            if (q + 1 == order.size()) {
-                if (ia < c->s) {
-                    const double h = c->as[2 * ia] + c->as[2 * ia + 1];
-                    ps.epi_cplx = rtab(c, RT_LENGTH, h, NO_COEF);
-                    for (int j = 0; j < c->dim; ++j) ps.ax_cplx[j] = field_slice(c, lst, ia, j);
-                } else {
-                    if (masked)
-                        for (int j = 0; j < c->dim; ++j) ps.ax_real[j] = c->mask_dev[j].p;
-                    if (!fin.empty()) ps.red = fin[0];
-                }
+            if (q == 0 && ia > 0) {
+                const double h = c->as[2 * (ia - 1)] + c->as[2 * (ia - 1) + 1];
+                ps.pro_cplx = rtab(c, RT_LENGTH, h, NO_COEF);
+                for (int j = 0; j < c->dim; ++j) ps.ax_cplx[j] = field_slice(c, lst, ia - 1, j);
+                ps.ax_in_prologue = 1;
+            }
+            if (q + 1 == order.size() && ia == c->s) {
+                if (masked)
+                    for (int j = 0; j < c->dim; ++j) ps.ax_real[j] = c->mask_dev[j].p;
+                if (!fin.empty()) ps.red = fin[0];
             }
             launch_pass(c, ps);
         }
@@ -769,22 +802,19 @@ static void length_step(qnd_ctx* c, void* psi, int64_t lst, const std::vector<Re
 static void velocity_step(qnd_ctx* c, void* psi, int64_t lst, const std::vector<RedDesc>& fin, bool masked) {
     auto order = pass_order(c);
     for (int ia = 0; ia < c->s; ++ia) {
-        const double a = c->as[2 * ia], b = c->as[2 * ia + 1];
         for (size_t q = 0; q < order.size(); ++q) {
             PassSpec ps;
             ps.axis = order[q];
             ps.psi = psi;
             ps.spec = field_slice(c, lst, ia, order[q]);
-            if (q == 0 && ia == 0) ps.pro_cplx = rtab(c, RT_VEL, a, NO_COEF);
-            if (q + 1 == order.size()) {
-                if (ia + 1 < c->s) {
-                    ps.epi_cplx = rtab(c, RT_VEL, b, c->as[2 * ia + 2]);
-                } else {
-                    ps.epi_cplx = rtab(c, RT_VEL, b, NO_COEF);
-                    if (masked)
-                        for (int j = 0; j < c->dim; ++j) ps.ax_real[j] = c->mask_dev[j].p;
-                    if (!fin.empty()) ps.red = fin[0];
-                }
+            if (q == 0)
+                ps.pro_cplx = ia == 0 ? rtab(c, RT_VEL, c->as[0], NO_COEF)
+                                      : rtab(c, RT_VEL, c->as[2 * ia - 1], c->as[2 * ia]);
+            if (q + 1 == order.size() && ia + 1 == c->s) {
+                ps.epi_cplx = rtab(c, RT_VEL, c->as[2 * c->s - 1], NO_COEF);
+                if (masked)
+                    for (int j = 0; j < c->dim; ++j) ps.ax_real[j] = c->mask_dev[j].p;
+                if (!fin.empty()) ps.red = fin[0];
             }
             launch_pass(c, ps);
         }
@@ -993,6 +1023,8 @@ static void build_context(qnd_ctx* c, int dim, const int64_t* nr, const double* 
     }
     c->axtot = off;
     QND_CK(cudaGetDevice(&c->device));
+    QND_CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
+    if (const char* e = getenv("QND_PDL")) c->pdl = atoi(e) != 0;
     QND_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     c->own_stream = true;
     std::vector<double> rall, pall;
@@ -1000,8 +1032,8 @@ static void build_context(qnd_ctx* c, int dim, const int64_t* nr, const double* 
         rall.insert(rall.end(), c->r[j].begin(), c->r[j].end());
         pall.insert(pall.end(), c->p[j].begin(), c->p[j].end());
     }
-    upload_f64(c->r_dev, rall);
-    upload_f64(c->p_dev, pall);
+    upload_f64(c, c->r_dev, rall);
+    upload_f64(c, c->p_dev, pall);
     for (int j = 0; j < dim; ++j) build_twiddles(c, j);
 }
 
@@ -1190,7 +1222,7 @@ int qnd_set_gradv(qnd_ctx* ctx, int axis, const double* gradv_host) {
         ctx->gradv_dev[axis].reset();
     } else {
         ctx->gradv[axis].assign(gradv_host, gradv_host + ctx->n);
-        upload_f64(ctx->gradv_dev[axis], ctx->gradv[axis]);
+        upload_f64(ctx, ctx->gradv_dev[axis], ctx->gradv[axis]);
     }
     QND_API_END
 }

@@ -45,37 +45,55 @@ template <typename V, typename S> __device__ __forceinline__ V cscale(V a, S s) 
 
 __host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
 
-// Correctly rounded cos/sin of pi/4 and pi/8 (exact mathematical constants).
-#define QND_R2 0.7071067811865476
-#define QND_C8 0.9238795325112867
-#define QND_S8 0.3826834323650898
+// Correctly rounded cos(k*pi/16), k = 0..8 (exact mathematical constants; sin(k*pi/16) = cos((8-k)*pi/16)).
+__host__ __device__ constexpr double cos_pi16(int k) {
+    return k == 0 ? 1.0
+         : k == 1 ? 0.9807852804032304
+         : k == 2 ? 0.9238795325112867
+         : k == 3 ? 0.8314696123025452
+         : k == 4 ? 0.7071067811865476
+         : k == 5 ? 0.5555702330196022
+         : k == 6 ? 0.3826834323650898
+         : k == 7 ? 0.19509032201612828
+         : 0.0;
+}
 
-// Multiply a by exp(SIGN * 2*pi*i*K/N) for N <= 16, with the trivial angles special-cased.
+// Multiply a by exp(SIGN * 2*pi*i*K/N) for N <= 32, with the trivial angles special-cased.
 template <int N, int K, int SIGN, typename V> __device__ __forceinline__ V twiddle_const(V a) {
     using S = decltype(a.x);
+    static_assert(32 % N == 0, "twiddle_const handles N <= 32");
     constexpr int k = ((K % N) + N) % N;
-    constexpr int e = k * (16 / N);  // angle in units of 2*pi/16
-    static_assert(16 % N == 0, "twiddle_const handles N <= 16");
+    constexpr int e = k * (32 / N);  // angle in units of 2*pi/32
     if constexpr (e == 0) {
         return a;
-    } else if constexpr (e == 8) {
+    } else if constexpr (e == 16) {
         return V{-a.x, -a.y};
-    } else if constexpr (e == 4 || e == 12) {
+    } else if constexpr (e == 8 || e == 24) {
         // exp(+-i*pi/2) = +-i ; (x+iy)*i = -y+ix
-        constexpr int s = (e == 4 ? 1 : -1) * SIGN;
+        constexpr int s = (e == 8 ? 1 : -1) * SIGN;
         if constexpr (s > 0) return V{-a.y, a.x};
         else return V{a.y, -a.x};
     } else {
-        // general angle: cos/sin from the pi/8 table with exact symmetry
-        constexpr int q = e % 4;  // 1,2,3 within the quadrant
-        constexpr int quad = e / 4;
-        constexpr double c0 = q == 1 ? QND_C8 : (q == 2 ? QND_R2 : QND_S8);
-        constexpr double s0 = q == 1 ? QND_S8 : (q == 2 ? QND_R2 : QND_C8);
+        constexpr int r = e % 8, quad = e / 8;
+        constexpr double c0 = cos_pi16(r), s0 = cos_pi16(8 - r);
         // rotate (c0, s0) by quad * pi/2
         constexpr double c = quad == 0 ? c0 : (quad == 1 ? -s0 : (quad == 2 ? -c0 : s0));
         constexpr double sn = quad == 0 ? s0 : (quad == 1 ? c0 : (quad == 2 ? -s0 : -c0));
-        const S cw = S(c), sw = S(SIGN * sn);
-        return V{a.x * cw - a.y * sw, a.x * sw + a.y * cw};
+        if constexpr (sizeof(S) == 4) {
+            // A float pair (cos, sin) has |w|^2 != 1 by a fixed amount, and since the same constants
+            // are used in every butterfly that bias would accumulate into a steady drift of the norm.
+            // Apply each constant as hi + lo (double-float) so the product is accurate to well below
+            // float rounding; the remaining error is the unbiased rounding of the result.
+            constexpr float chi = float(c), clo = float(c - double(float(c)));
+            constexpr double sd = SIGN * sn;
+            constexpr float shi = float(sd), slo = float(sd - double(float(sd)));
+            const float re = __fmaf_rn(a.x, chi, __fmaf_rn(-a.y, shi, a.x * clo - a.y * slo));
+            const float im = __fmaf_rn(a.x, shi, __fmaf_rn(a.y, chi, a.x * slo + a.y * clo));
+            return V{re, im};
+        } else {
+            const S cw = S(c), sw = S(SIGN * sn);
+            return V{a.x * cw - a.y * sw, a.x * sw + a.y * cw};
+        }
     }
 }
 
@@ -113,8 +131,9 @@ template <int SIGN> struct RegDFT<2, SIGN> {
     }
 };
 
-// Shared-memory index with one pad slot per 16 values.
-__device__ __forceinline__ int spad(int i) { return i + (i >> 4); }
+// Shared-memory index with one pad slot per E values (E = values per thread): the first stage
+// writes E*tid + r, which the pad spreads over consecutive banks.
+template <int E> __device__ __forceinline__ int spad(int i) { return i + (i >> ilog2(E)); }
 
 // Compile-time description of the stage sequence for a length-L line with E values per thread.
 template <int L, int E> struct FFTPlan {
@@ -131,13 +150,15 @@ template <int L, int E> struct FFTPlan {
         return st <= 1 ? 0 : tw_offset(st - 1) + span(st - 1) * (radix(st - 1) - 1);
     }
     __host__ __device__ static constexpr int tw_size() { return tw_offset(NSTAGE) ; }
-    static constexpr int SMEM_LINE = L >= 16 ? L + L / 16 : L;  // padded values per line (before line padding)
+    static constexpr int SMEM_LINE = L + L / E;  // padded values per line (before line padding)
 };
 
 // One Stockham stage on the thread's E registers (B = E/R butterflies, j = tid + b*T).
 // Input registers hold x[j + r*L/R] for butterfly b at v[b*R + r]; output registers hold
 // the butterfly outputs in the same slots. Twiddles come from smem table tw (forward sign).
-template <int L, int E, int ST, int SIGN, typename V>
+// TWS: the twiddle table lives in shared memory (plain loads) rather than global memory
+// (read-only cache loads; never use those on a shared-memory address).
+template <int L, int E, int ST, int SIGN, bool TWS, typename V>
 __device__ __forceinline__ void fft_stage_regs(V* v, int tid, const V* __restrict__ tw) {
     using P = FFTPlan<L, E>;
     constexpr int R = P::radix(ST);
@@ -152,7 +173,9 @@ __device__ __forceinline__ void fft_stage_regs(V* v, int tid, const V* __restric
             const V* t = tw + P::tw_offset(ST) + jm * (R - 1);
 #pragma unroll
             for (int r = 1; r < R; ++r) {
-                V w = t[r - 1];
+                V w;
+                if constexpr (TWS) w = t[r - 1];
+                else w = __ldg(t + r - 1);
                 if constexpr (SIGN > 0) w.y = -w.y;
                 u[r] = cmul(u[r], w);
             }
@@ -175,35 +198,42 @@ template <int L, int E> struct SlotMap {
 // Full FFT of one line held in registers: on entry v[u] = x[tid + u*T], on exit
 // v[u] = X[tid + u*T] (both in natural slots). `line` is this line's padded smem
 // buffer; `sync` is the CTA barrier (all lines of a CTA transform in lockstep).
-// Call as fft_line_stages<L, E, SIGN, 0>(...).
-template <int L, int E, int SIGN, int ST, typename V, typename Sync>
+// Call as fft_line_stages<L, E, SIGN, 0, TWS>(...).
+template <int L, int E, int SIGN, int ST, bool TWS, typename V, typename Sync>
 __device__ __forceinline__ void fft_line_stages(V* v, int tid, V* line, const V* __restrict__ tw, Sync sync) {
     using P = FFTPlan<L, E>;
     constexpr int T = P::T;
     constexpr int R = P::radix(ST);
     constexpr int Ns = P::span(ST);
     constexpr int B = E / R;
-    fft_stage_regs<L, E, ST, SIGN>(v, tid, tw);
+    fft_stage_regs<L, E, ST, SIGN, TWS>(v, tid, tw);
     if constexpr (ST + 1 < P::NSTAGE) {
-        // exchange: store outputs of stage ST, load inputs of stage ST+1
+        // Exchange: store the outputs of stage ST, load the inputs of stage ST+1. Every stride used
+        // here (Ns for the stores, L/R2 for the loads) is 1 with an E-aligned base (first stage) or a
+        // multiple of E, so spad(base + r*step) = spad(base) + r*(step + step/E): one padded base per
+        // butterfly and compile-time offsets after it.
         constexpr int R2 = P::radix(ST + 1);
         constexpr int B2 = E / R2;
+        constexpr int SP = Ns == 1 ? 1 : Ns + Ns / E;                 // padded store stride
+        constexpr int LP = (L / R2) + (L / R2) / E;                   // padded load stride
+        static_assert(Ns == 1 || Ns % E == 0, "stage spans are multiples of E");
+        static_assert((L / R2) % E == 0, "load strides are multiples of E");
 #pragma unroll
         for (int b = 0; b < B; ++b) {
             const int j = tid + b * T;
-            const int base = (j / Ns) * Ns * R + (j & (Ns - 1));
+            V* p = line + spad<E>((j / Ns) * Ns * R + (j & (Ns - 1)));
 #pragma unroll
-            for (int r = 0; r < R; ++r) line[spad(base + r * Ns)] = v[b * R + r];
+            for (int r = 0; r < R; ++r) p[r * SP] = v[b * R + r];
         }
         sync();
 #pragma unroll
         for (int b = 0; b < B2; ++b) {
-            const int j = tid + b * T;
+            const V* p = line + spad<E>(tid + b * T);
 #pragma unroll
-            for (int r = 0; r < R2; ++r) v[b * R2 + r] = line[spad(j + r * (L / R2))];
+            for (int r = 0; r < R2; ++r) v[b * R2 + r] = p[r * LP];
         }
         sync();
-        fft_line_stages<L, E, SIGN, ST + 1>(v, tid, line, tw, sync);
+        fft_line_stages<L, E, SIGN, ST + 1, TWS>(v, tid, line, tw, sync);
     } else {
         // last stage: outputs at positions j + r*Ns (j = tid + b*T < Ns); reorder registers to
         // natural slots v[u] = X[tid + u*T].

@@ -11,6 +11,7 @@ struct PassKernelInfo {
     size_t smem;  // dynamic shared memory bytes
     int G;        // lines per CTA
     int tw_size;  // twiddle entries expected in the plan table
+    int E;        // values per thread (fixes the stage structure of the twiddle table)
 };
 
 // Defined once per line length in qnd_pass_inst.cu (compiled with -DQND_L=...).
@@ -21,8 +22,8 @@ struct HostPlan {
     int L, E, T, nstage;
     int radix[16], span[16];
     int tw_size;
-    explicit HostPlan(int L_) : L(L_) {
-        E = L < 16 ? L : 16;
+    HostPlan(int L_, int E_) : L(L_) {
+        E = E_;
         T = L / E;
         int logl = 0, loge = 0;
         while ((1 << logl) < L) ++logl;
