@@ -135,7 +135,8 @@ struct qnd_ctx {
 
     DevBuf tw[MAX_DIM];
     DevBuf r_dev, p_dev;  // concatenated axes (double)
-    DevBuf gradv_dev[MAX_DIM];
+    DevBuf gradv_dev[MAX_DIM];                // natural layout
+    DevBuf gradv_lm[MAX_DIM][MAX_DIM];        // [component][pass axis] line-major copies
     DevBuf mask_dev[MAX_DIM];
     DevBuf vpot_dev;      // double, for the energy operator
     std::map<std::tuple<int, int, double, double>, std::unique_ptr<DevBuf>> spec_cache;
@@ -276,8 +277,31 @@ static inline double clamped_exp(double arg) { return std::exp(arg > MAX_EXP_ARG
 //   RT_IMAG   (a[, b]):  exp(min(700, -a V)) [* exp(min(700, -b V))]           real (integrators.c:143-160)
 //   RT_LENGTH (h):       exp(min(700, -h Vcap)) exp(-i h V)                      complex (integrators.c:186-188)
 //   RT_VEL    (a[, b]):  exp(min(700,-a Vcap)) exp(-i a V) [* same with b]       complex (integrators.c:209-229)
-static const void* rtab(qnd_ctx* c, int kind, double a, double b) {
-    auto key = std::make_tuple(kind, a, b, c->table_epoch);
+// Reorder a full-grid array (comps values per point) to line-major order for axis ax: entry
+// lam*L + m holds point m of line lam (the order in which a pass along ax visits the grid).
+static std::vector<double> line_major(const qnd_ctx* c, const std::vector<double>& nat, int comps, int ax) {
+    if (ax == c->dim - 1) return nat;
+    const int64_t L = c->nr[ax];
+    const int log2S = c->shift[ax];
+    const int64_t S = int64_t(1) << log2S, nlines = c->n / L;
+    std::vector<double> out(nat.size());
+    for (int64_t lam = 0; lam < nlines; ++lam) {
+        const int64_t base = ((lam >> log2S) * L << log2S) + (lam & (S - 1));
+        for (int64_t m = 0; m < L; ++m) {
+            const int64_t src = (base + (m << log2S)) * comps, dst = (lam * L + m) * comps;
+            for (int q = 0; q < comps; ++q) out[dst + q] = nat[src + q];
+        }
+    }
+    return out;
+}
+
+static const void* rtab(qnd_ctx* c, int kind, double a, double b, int ax);
+
+// Full-grid tables in the natural layout (the contiguous axis' line-major layout).
+static const void* rtab(qnd_ctx* c, int kind, double a, double b) { return rtab(c, kind, a, b, c->dim - 1); }
+
+static const void* rtab(qnd_ctx* c, int kind, double a, double b, int ax) {
+    auto key = std::make_tuple(kind * 8 + ax, a, b, c->table_epoch);
     auto it = c->rtab_cache.find(key);
     if (it != c->rtab_cache.end()) return it->second->p;
     if (c->vpot.empty()) QND_FAIL(QND_EINVAL, "no potential set: call qnd_set_potential_named or qnd_set_potential");
@@ -290,7 +314,7 @@ static const void* rtab(qnd_ctx* c, int kind, double a, double b) {
             if (b != NO_COEF) f *= clamped_exp(-b * c->vpot[i]);
             v[i] = f;
         }
-        upload_real(c, *buf, v);
+        upload_real(c, *buf, line_major(c, v, 1, ax));
     } else {
         std::vector<double> v(2 * n);
         for (size_t i = 0; i < n; ++i) {
@@ -315,7 +339,7 @@ static const void* rtab(qnd_ctx* c, int kind, double a, double b) {
             v[2 * i] = re;
             v[2 * i + 1] = im;
         }
-        upload_cplx(c, *buf, v);
+        upload_cplx(c, *buf, line_major(c, v, 2, ax));
     }
     const void* ptr = buf->p;
     c->rtab_cache[key] = std::move(buf);
@@ -339,6 +363,10 @@ struct PassSpec {
     const void* pro_cplx = nullptr;
     const double* pro_scale = nullptr;
     const void* spec = nullptr;
+    const void* spec2 = nullptr;
+    const void* mid_real = nullptr;
+    const void* mid_cplx = nullptr;
+    const void* mid_ax_cplx[MAX_DIM] = {nullptr, nullptr, nullptr};
     const void* epi_real = nullptr;
     const void* epi_cplx = nullptr;
     const void* ax_cplx[MAX_DIM] = {nullptr, nullptr, nullptr};
@@ -375,6 +403,10 @@ template <typename R> static void fill_args(qnd_ctx* c, const PassSpec& ps, Pass
     a.pro_cplx = static_cast<const V*>(ps.pro_cplx);
     a.pro_scale_dev = ps.pro_scale;
     a.spec = static_cast<const V*>(ps.spec);
+    a.spec2 = static_cast<const V*>(ps.spec2);
+    a.mid_real = static_cast<const R*>(ps.mid_real);
+    a.mid_cplx = static_cast<const V*>(ps.mid_cplx);
+    for (int k = 0; k < MAX_DIM; ++k) a.mid_ax_cplx[k] = static_cast<const V*>(ps.mid_ax_cplx[k]);
     a.epi_real = static_cast<const R*>(ps.epi_real);
     a.epi_cplx = static_cast<const V*>(ps.epi_cplx);
     for (int k = 0; k < MAX_DIM; ++k) {
@@ -535,7 +567,16 @@ static bool all_rspace(const std::vector<ObsItem>& items) {
 
 // Reductions of |psi|^2 for the r-space observables, writing into row (the contiguous
 // outputs must be adjacent: r-space items are emitted in one descriptor per contiguous run).
-static std::vector<RedDesc> rspace_red(qnd_ctx* c, const std::vector<ObsItem>& items, double* row) {
+// dV/dx_j laid out line-major for pass axis ax (the natural array when ax is the last axis).
+static const double* gradv_layout(qnd_ctx* c, int j, int ax) {
+    if (ax == c->dim - 1) return c->gradv_dev[j].as<double>();
+    DevBuf& b = c->gradv_lm[j][ax];
+    if (!b.p) upload_f64(c, b, line_major(c, c->gradv[j], 1, ax));
+    return b.as<double>();
+}
+
+// lm_axis: the pass axis whose line-major order the fused reduction visits (dim-1: natural).
+static std::vector<RedDesc> rspace_red(qnd_ctx* c, const std::vector<ObsItem>& items, double* row, int lm_axis) {
     std::vector<RedDesc> out;
     RedDesc cur{};
     int cur_off = -1;
@@ -562,7 +603,7 @@ static std::vector<RedDesc> rspace_red(qnd_ctx* c, const std::vector<ObsItem>& i
         else if (it.kind == OB_DIPOLE_R)
             for (int j = 0; j < c->dim; ++j) add(it.offset + j, RK_ABS2, WK_AXIS, j, c->r_dev.as<double>() + c->axoff[j], c->dNr);
         else if (it.kind == OB_ACCEL)
-            for (int j = 0; j < c->dim; ++j) add(it.offset + j, RK_ABS2, WK_GRID, 0, c->gradv_dev[j].as<double>(), -c->dNr);
+            for (int j = 0; j < c->dim; ++j) add(it.offset + j, RK_ABS2, WK_GRID, 0, gradv_layout(c, j, lm_axis), -c->dNr);
     }
     flush();
     return out;
@@ -611,7 +652,7 @@ static void energy_moments(qnd_ctx* c, const void* psi, int nmom, double* out_de
 // Evaluate observables of an r-space psi into the device row (calculate_observables.c:119-140).
 static void eval_obs(qnd_ctx* c, const void* psi, const std::vector<ObsItem>& items, const double* alpha,
                      double* row_dev) {
-    for (auto& rd : rspace_red(c, items, row_dev)) grid_reduce(c, psi, rd);
+    for (auto& rd : rspace_red(c, items, row_dev, c->dim - 1)) grid_reduce(c, psi, rd);
     for (auto& it : items) {
         if (it.kind == OB_DIPOLE_V) {
             // sum_k |psi~|^2 (p_j + alpha_j) dNp fft_scaling = (dNp/N_j) sum |F_j psi|^2 (p_j + alpha_j)
@@ -695,32 +736,6 @@ static void check_imag_clamp(qnd_ctx* c) {
     }
 }
 
-// Integration_step_imag x nsteps on an r-space psi (integrators.c:135-163). pro_scale (device scalar,
-// may be null) multiplies psi before the first step (deferred Gram-Schmidt normalisation).
-static void imag_steps(qnd_ctx* c, void* psi, int64_t nsteps, const double* pro_scale) {
-    check_imag_clamp(c);
-    auto order = pass_order(c);
-    for (int64_t st = 0; st < nsteps; ++st) {
-        for (int ia = 0; ia < c->s; ++ia) {
-            const double h = c->as[2 * ia] + c->as[2 * ia + 1];
-            for (size_t q = 0; q < order.size(); ++q) {
-                PassSpec ps;
-                ps.axis = order[q];
-                ps.psi = psi;
-                ps.spec = spec_table(c, SP_IMAG, order[q], h);
-                if (q == 0) {
-                    // factors before K(h_ia): V(a_0) at the start, V(a_{2ia-1}) V(a_{2ia}) in between
-                    ps.pro_real = ia == 0 ? rtab(c, RT_IMAG, c->as[0], NO_COEF)
-                                          : rtab(c, RT_IMAG, c->as[2 * ia - 1], c->as[2 * ia]);
-                    if (ia == 0 && st == 0) ps.pro_scale = pro_scale;
-                }
-                if (q + 1 == order.size() && ia + 1 == c->s) ps.epi_real = rtab(c, RT_IMAG, c->as[2 * c->s - 1], NO_COEF);
-                launch_pass(c, ps);
-            }
-        }
-    }
-}
-
 // Per-step field tables (laser phases / velocity-gauge kinetic phases) for a chunk of steps
 // from field samples already on the device.
 static void build_field_tables(qnd_ctx* c, const double* field_dev, int64_t nsteps, bool velocity) {
@@ -762,64 +777,153 @@ static bool has_mask(const qnd_ctx* c) {
     return false;
 }
 
-// One length-gauge step in r-space (chunk-local step index lst for the field tables).
-// fin: reductions fused into the final pass (may be empty); masked: apply the step mask.
-// Each kinetic sandwich runs the contiguous axis first; the potential/laser factor V(h) that
-// separates two sandwiches is applied as the prologue of the next sandwich's first pass, where
-// its full-grid table is read with coalesced accesses alongside the state.
-static void length_step(qnd_ctx* c, void* psi, int64_t lst, const std::vector<RedDesc>& fin, bool masked) {
-    auto order = pass_order(c);
-    for (int ia = 0; ia <= c->s; ++ia) {
-        // kinetic sandwich before V(h_ia): K(a_0) first, K(a_{2ia-1} + a_{2ia}) between, K(a_{2s-1}) last
-        double kc;
-        if (ia == 0) kc = c->as[0];
-        else if (ia == c->s) kc = c->as[2 * c->s - 1];
-        else kc = c->as[2 * ia - 1] + c->as[2 * ia];
-        for (size_t q = 0; q < order.size(); ++q) {
+// ---------------------------------------------------------------- sandwich chains --
+//
+// A split-operator step is a chain of kinetic sandwiches K_0 .. K_{NK-1} (each a product of one
+// pass per axis) with point-wise r-space factors M_i between K_i and K_{i+1}, an optional factor
+// before K_0 and one after K_{NK-1}. Consecutive sandwiches run their axes in opposite orders, so
+// the last axis of K_i is the first axis of K_{i+1}: those two axis passes and M_i fuse into one
+// PM_DOUBLE pass. A 2-D step costs NK + 1 passes instead of 2 NK; a 3-D step 2 NK + 1 instead of
+// 3 NK; in 1-D the sandwiches pair up two per pass.
+
+struct Factor {
+    int kind = -1;        // RT_IMAG (real table), RT_LENGTH / RT_VEL (complex), -1: none
+    double a = 0.0, b = NO_COEF;
+    int laser_ia = -1;    // length gauge: per-axis laser phases of sub-step laser_ia
+};
+
+static void set_factor(qnd_ctx* c, const Factor& f, int ax, int64_t lst, const void** treal, const void** tcplx,
+                       const void** axc) {
+    if (f.kind >= 0) {
+        const void* p = rtab(c, f.kind, f.a, f.b, ax);
+        if (f.kind == RT_IMAG) *treal = p;
+        else *tcplx = p;
+    }
+    if (f.laser_ia >= 0 && axc)
+        for (int j = 0; j < c->dim; ++j) axc[j] = field_slice(c, lst, f.laser_ia, j);
+}
+
+// Axis of the chain's last pass (the one that carries the final factor, mask and reductions).
+static int chain_final_axis(const qnd_ctx* c, int NK) {
+    if (c->dim == 1) return 0;
+    return ((NK - 1) % 2 == 0) ? 0 : c->dim - 1;
+}
+
+template <class SpecFn, class MidFn>
+static void sandwich_chain(qnd_ctx* c, void* psi, int NK, SpecFn spec_of, MidFn mid_of, const Factor& pre,
+                           const double* pre_scale, const Factor& post, bool masked, const RedDesc* fin,
+                           int64_t lst) {
+    const int d = c->dim;
+    auto finish = [&](PassSpec& ps) {
+        set_factor(c, post, ps.axis, lst, &ps.epi_real, &ps.epi_cplx, nullptr);
+        if (masked)
+            for (int j = 0; j < d; ++j) ps.ax_real[j] = c->mask_dev[j].p;
+        if (fin) ps.red = *fin;
+    };
+    if (d == 1) {
+        int i = 0;
+        while (i < NK) {
             PassSpec ps;
-            ps.axis = order[q];
+            ps.axis = 0;
             ps.psi = psi;
-            ps.spec = spec_table(c, SP_LENGTH, order[q], kc);
-            if (q == 0 && ia > 0) {
-                const double h = c->as[2 * (ia - 1)] + c->as[2 * (ia - 1) + 1];
-                ps.pro_cplx = rtab(c, RT_LENGTH, h, NO_COEF);
-                for (int j = 0; j < c->dim; ++j) ps.ax_cplx[j] = field_slice(c, lst, ia - 1, j);
-                ps.ax_in_prologue = 1;
+            ps.spec = spec_of(i, 0);
+            const Factor before = i == 0 ? pre : mid_of(i - 1);
+            set_factor(c, before, 0, lst, &ps.pro_real, &ps.pro_cplx, ps.ax_cplx);
+            if (before.laser_ia >= 0) ps.ax_in_prologue = 1;
+            if (i == 0) ps.pro_scale = pre_scale;
+            if (i + 1 < NK) {
+                ps.mode = PM_DOUBLE;
+                set_factor(c, mid_of(i), 0, lst, &ps.mid_real, &ps.mid_cplx, ps.mid_ax_cplx);
+                ps.spec2 = spec_of(i + 1, 0);
+                i += 2;
+            } else {
+                i += 1;
             }
-            if (q + 1 == order.size() && ia == c->s) {
-                if (masked)
-                    for (int j = 0; j < c->dim; ++j) ps.ax_real[j] = c->mask_dev[j].p;
-                if (!fin.empty()) ps.red = fin[0];
+            if (i >= NK) finish(ps);
+            launch_pass(c, ps);
+        }
+        return;
+    }
+    for (int i = 0; i < NK; ++i) {
+        for (int q = (i > 0 ? 1 : 0); q < d; ++q) {
+            const int ax = (i % 2 == 0) ? d - 1 - q : q;
+            PassSpec ps;
+            ps.axis = ax;
+            ps.psi = psi;
+            ps.spec = spec_of(i, ax);
+            if (i == 0 && q == 0) {
+                set_factor(c, pre, ax, lst, &ps.pro_real, &ps.pro_cplx, ps.ax_cplx);
+                if (pre.laser_ia >= 0) ps.ax_in_prologue = 1;
+                ps.pro_scale = pre_scale;
             }
+            if (q == d - 1 && i + 1 < NK) {
+                ps.mode = PM_DOUBLE;
+                set_factor(c, mid_of(i), ax, lst, &ps.mid_real, &ps.mid_cplx, ps.mid_ax_cplx);
+                ps.spec2 = spec_of(i + 1, ax);
+            }
+            if (q == d - 1 && i + 1 == NK) finish(ps);
             launch_pass(c, ps);
         }
     }
-    // further reduction descriptors (more than one run of outputs) read the final state again
-    for (size_t k = 1; k < fin.size(); ++k) grid_reduce(c, psi, fin[k]);
+}
+
+// Integration_step_imag x nsteps on an r-space psi (integrators.c:135-163): V(a_0) K(h_0) V(a_1)V(a_2)
+// K(h_1) ... K(h_{s-1}) V(a_{2s-1}). pro_scale (device scalar, may be null) multiplies psi before the
+// first step (the deferred Gram-Schmidt normalisation).
+static void imag_steps(qnd_ctx* c, void* psi, int64_t nsteps, const double* pro_scale) {
+    check_imag_clamp(c);
+    for (int64_t st = 0; st < nsteps; ++st) {
+        auto spec_of = [&](int i, int ax) { return spec_table(c, SP_IMAG, ax, c->as[2 * i] + c->as[2 * i + 1]); };
+        auto mid_of = [&](int i) {
+            Factor f;
+            f.kind = RT_IMAG;
+            f.a = c->as[2 * i + 1];
+            f.b = c->as[2 * i + 2];
+            return f;
+        };
+        Factor pre, post;
+        pre.kind = post.kind = RT_IMAG;
+        pre.a = c->as[0];
+        post.a = c->as[2 * c->s - 1];
+        sandwich_chain(c, psi, c->s, spec_of, mid_of, pre, st == 0 ? pro_scale : nullptr, post, false, nullptr, 0);
+    }
+}
+
+// One length-gauge step in r-space (integrators.c:170-194 rewritten in r-space; chunk-local step
+// index lst for the field tables): K(a_0) V(h_0) K(a_1 + a_2) V(h_1) ... V(h_{s-1}) K(a_{2s-1}), then
+// the step mask and the fused reductions `fin` (of psi(t_{n+1})).
+static void length_step(qnd_ctx* c, void* psi, int64_t lst, const RedDesc* fin, bool masked) {
+    auto kc = [&](int i) {
+        if (i == 0) return c->as[0];
+        if (i == c->s) return c->as[2 * c->s - 1];
+        return c->as[2 * i - 1] + c->as[2 * i];
+    };
+    auto spec_of = [&](int i, int ax) { return spec_table(c, SP_LENGTH, ax, kc(i)); };
+    auto mid_of = [&](int i) {
+        Factor f;
+        f.kind = RT_LENGTH;
+        f.a = c->as[2 * i] + c->as[2 * i + 1];
+        f.laser_ia = i;
+        return f;
+    };
+    sandwich_chain(c, psi, c->s + 1, spec_of, mid_of, Factor{}, nullptr, Factor{}, masked, fin, lst);
 }
 
 // One velocity-gauge step in r-space (integrators.c:201-232).
-static void velocity_step(qnd_ctx* c, void* psi, int64_t lst, const std::vector<RedDesc>& fin, bool masked) {
-    auto order = pass_order(c);
-    for (int ia = 0; ia < c->s; ++ia) {
-        for (size_t q = 0; q < order.size(); ++q) {
-            PassSpec ps;
-            ps.axis = order[q];
-            ps.psi = psi;
-            ps.spec = field_slice(c, lst, ia, order[q]);
-            if (q == 0)
-                ps.pro_cplx = ia == 0 ? rtab(c, RT_VEL, c->as[0], NO_COEF)
-                                      : rtab(c, RT_VEL, c->as[2 * ia - 1], c->as[2 * ia]);
-            if (q + 1 == order.size() && ia + 1 == c->s) {
-                ps.epi_cplx = rtab(c, RT_VEL, c->as[2 * c->s - 1], NO_COEF);
-                if (masked)
-                    for (int j = 0; j < c->dim; ++j) ps.ax_real[j] = c->mask_dev[j].p;
-                if (!fin.empty()) ps.red = fin[0];
-            }
-            launch_pass(c, ps);
-        }
-    }
-    for (size_t k = 1; k < fin.size(); ++k) grid_reduce(c, psi, fin[k]);
+static void velocity_step(qnd_ctx* c, void* psi, int64_t lst, const RedDesc* fin, bool masked) {
+    auto spec_of = [&](int i, int ax) { return field_slice(c, lst, i, ax); };
+    auto mid_of = [&](int i) {
+        Factor f;
+        f.kind = RT_VEL;
+        f.a = c->as[2 * i + 1];
+        f.b = c->as[2 * i + 2];
+        return f;
+    };
+    Factor pre, post;
+    pre.kind = post.kind = RT_VEL;
+    pre.a = c->as[0];
+    post.a = c->as[2 * c->s - 1];
+    sandwich_chain(c, psi, c->s, spec_of, mid_of, pre, nullptr, post, masked, fin, lst);
 }
 
 static void unitary_fft(qnd_ctx* c, void* psi, bool forward) {
@@ -861,9 +965,15 @@ static void run_realtime(qnd_ctx* c, void* psi, const double* field_host, const 
             const int64_t gst = c0 + k;
             double* row = rows + size_t(k + 1) * nv;
             std::vector<RedDesc> fin;
-            if (nv > 0 && (fused || fused_v)) fin = rspace_red(c, items, row);
-            if (velocity) velocity_step(c, psi, k, fin, masked);
-            else length_step(c, psi, k, fin, masked);
+            const int NK = velocity ? c->s : c->s + 1;
+            if (nv > 0 && (fused || fused_v)) fin = rspace_red(c, items, row, chain_final_axis(c, NK));
+            const RedDesc* f0 = fin.empty() ? nullptr : &fin[0];
+            if (velocity) velocity_step(c, psi, k, f0, masked);
+            else length_step(c, psi, k, f0, masked);
+            if (fin.size() > 1) {  // outputs beyond the first descriptor: a read of the final state
+                auto nat = rspace_red(c, items, row, c->dim - 1);
+                for (size_t q = 1; q < nat.size(); ++q) grid_reduce(c, psi, nat[q]);
+            }
             if (nv > 0 && !(fused || fused_v) && gst + 1 < nsteps) {
                 const double* al = velocity ? alpha_host + size_t(gst + 1) * c->dim : zero_alpha.data();
                 eval_obs(c, psi, items, al, row);
@@ -1220,9 +1330,11 @@ int qnd_set_gradv(qnd_ctx* ctx, int axis, const double* gradv_host) {
     if (!gradv_host) {
         ctx->gradv[axis].clear();
         ctx->gradv_dev[axis].reset();
+        for (int k = 0; k < MAX_DIM; ++k) ctx->gradv_lm[axis][k].reset();
     } else {
         ctx->gradv[axis].assign(gradv_host, gradv_host + ctx->n);
         upload_f64(ctx, ctx->gradv_dev[axis], ctx->gradv[axis]);
+        for (int k = 0; k < MAX_DIM; ++k) ctx->gradv_lm[axis][k].reset();
     }
     QND_API_END
 }
@@ -1355,7 +1467,7 @@ int qnd_step_length(qnd_ctx* ctx, void* psi_p_dev, const double* E_host, int64_t
     for (int64_t c0 = 0; c0 < nsteps; c0 += CHUNK) {
         const int64_t ch = std::min(CHUNK, nsteps - c0);
         upload_field_chunk(ctx, E_host + size_t(c0) * ctx->s * ctx->dim, ch, false);
-        for (int64_t k = 0; k < ch; ++k) length_step(ctx, psi_p_dev, k, {}, false);
+        for (int64_t k = 0; k < ch; ++k) length_step(ctx, psi_p_dev, k, nullptr, false);
     }
     unitary_fft(ctx, psi_p_dev, true);
     QND_CK(cudaGetLastError());
@@ -1372,7 +1484,7 @@ int qnd_step_velocity(qnd_ctx* ctx, void* psi_dev, const double* A_host, int64_t
     for (int64_t c0 = 0; c0 < nsteps; c0 += CHUNK) {
         const int64_t ch = std::min(CHUNK, nsteps - c0);
         upload_field_chunk(ctx, A_host + size_t(c0) * ctx->s * ctx->dim, ch, true);
-        for (int64_t k = 0; k < ch; ++k) velocity_step(ctx, psi_dev, k, {}, false);
+        for (int64_t k = 0; k < ch; ++k) velocity_step(ctx, psi_dev, k, nullptr, false);
     }
     QND_CK(cudaGetLastError());
     QND_API_END
@@ -1471,8 +1583,12 @@ int qnd_run_length_dev(qnd_ctx* ctx, void* psi_r_dev, const double* E_dev, int64
         for (int64_t k = 0; k < ch; ++k) {
             double* row = nv > 0 ? obs_dev + size_t(c0 + k) * nv : nullptr;
             std::vector<RedDesc> fin;
-            if (nv > 0 && fused) fin = rspace_red(ctx, items, row);
-            length_step(ctx, psi_r_dev, k, fin, masked);
+            if (nv > 0 && fused) fin = rspace_red(ctx, items, row, chain_final_axis(ctx, ctx->s + 1));
+            length_step(ctx, psi_r_dev, k, fin.empty() ? nullptr : &fin[0], masked);
+            if (fin.size() > 1) {
+                auto nat = rspace_red(ctx, items, row, ctx->dim - 1);
+                for (size_t q = 1; q < nat.size(); ++q) grid_reduce(ctx, psi_r_dev, nat[q]);
+            }
             if (nv > 0 && !fused) eval_obs(ctx, psi_r_dev, items, zero, row);
         }
     }

@@ -11,6 +11,14 @@
 // Modes
 //   PM_SANDWICH  psi <- epi(x) . IFFT[ spec(k) . FFT[ pro(x) . psi ] ]   (+ reductions)
 //                The split-operator kernel/potential sub-steps: one read, one write.
+//   PM_DOUBLE    psi <- epi . IFFT spec2 FFT [ mid(x) . IFFT spec FFT [ pro . psi ] ]: two kinetic
+//                sandwiches along the same axis with the r-space factor between them, still one
+//                read and one write (consecutive sandwiches alternate their axis order so that
+//                the last axis of one is the first axis of the next).
+//
+// Full-grid tables (pro/mid/epi factors, WK_GRID weights) are stored LINE-MAJOR for the pass
+// axis: entry lam*L + m for element m of line lam. Reads are then coalesced on every axis; for
+// the contiguous axis this is the natural layout.
 //   PM_FFT_FWD / PM_FFT_INV   psi <- scale . (I)FFT[psi]   (representation changes)
 //   PM_SPECRED   reductions of |FFT psi|^2 weighted by k-space tables; no write
 //   PM_APPLY     u = IFFT[spec . FFT psi] (+ V psi) (+ dst); optional store into dst and
@@ -27,9 +35,9 @@ namespace qnd {
 constexpr int MAX_RED = 8;
 constexpr int MAX_DIM = 3;
 
-enum : int { PM_SANDWICH = 0, PM_FFT_FWD = 1, PM_FFT_INV = 2, PM_SPECRED = 3, PM_APPLY = 4, PM_NMODES = 5 };
+enum : int { PM_SANDWICH = 0, PM_FFT_FWD = 1, PM_FFT_INV = 2, PM_SPECRED = 3, PM_APPLY = 4, PM_DOUBLE = 5, PM_NMODES = 6 };
 enum : int { RK_ABS2 = 0, RK_BILIN = 1 };          // |v|^2 * w   or   Re(conj(partner) * v) * w
-enum : int { WK_ONE = 0, WK_AXIS = 1, WK_GRID = 2 }; // weight 1, table[idx_axis], table[flat]
+enum : int { WK_ONE = 0, WK_AXIS = 1, WK_GRID = 2 }; // weight 1, table[idx_axis], line-major table
 
 struct RedDesc {
     int n;                       // accumulators in use (0: no reduction)
@@ -60,6 +68,10 @@ template <typename R> struct PassArgs {
     const V* pro_cplx;
     const double* pro_scale_dev;
     const V* spec;
+    const V* spec2;              // PM_DOUBLE: the second sandwich's spectral factors
+    const R* mid_real;           // PM_DOUBLE: r-space factors between the two sandwiches
+    const V* mid_cplx;
+    const V* mid_ax_cplx[MAX_DIM];
     const R* epi_real;
     const V* epi_cplx;
     const V* ax_cplx[MAX_DIM];   // per-axis factors (laser phases, step mask) applied ...
@@ -78,9 +90,13 @@ template <typename R> struct PassArgs {
 //   Lines along a strided axis are staged through shared memory with cp.async so that the
 //   global accesses run over G neighbouring lines; the stage buffer is then the exchange space.
 template <typename R, int L> struct PassShape {
-    static constexpr int E = L <= 16 ? L : 16;
+    // FP64, L >= 1024: 32 values per thread (two radix-32 stages at L = 1024), one CTA per line, a
+    // single warp per line at L = 1024 (warp-synchronous exchanges). Otherwise 16 values per thread
+    // and 128-thread CTAs holding several lines.
+    static constexpr bool WIDE = false;  // 32 values per thread for long FP64 lines: measured slower (too few warps per SM)
+    static constexpr int E = L <= 16 ? L : (WIDE ? 32 : 16);
     static constexpr int T = L / E;
-    static constexpr int G = T >= 128 ? 1 : 128 / T;
+    static constexpr int G = WIDE ? 1 : (T >= 128 ? 1 : 128 / T);
     static constexpr int NT = T * G;
     static constexpr bool EXCHANGE = FFTPlan<L, E>::NSTAGE > 1;
     static constexpr int SLOTS = sizeof(R) == 8 ? 8 : 16;  // element slots per bank cycle (16 B / 8 B values)
@@ -89,11 +105,14 @@ template <typename R, int L> struct PassShape {
     static constexpr int LINE_RAW = FFTPlan<L, E>::SMEM_LINE;
     static constexpr int LS = LINE_RAW + ((LS_TARGET - LINE_RAW % SLOTS) % SLOTS + SLOTS) % SLOTS;
     static constexpr int TWN_RAW = (FFTPlan<L, E>::tw_size() + 1) & ~1;
-    static constexpr bool TW_SMEM = size_t(TWN_RAW) * sizeof(cplx_t<R>) <= 16 * 1024;  // stage twiddles in smem
+    // stage twiddles in shared memory when they are small and shared by several lines of the CTA;
+    // otherwise read them through L1 (one copy per SM instead of one per CTA)
+    static constexpr bool TW_SMEM = G > 1 && size_t(TWN_RAW) * sizeof(cplx_t<R>) <= 16 * 1024;
     static constexpr int TWN = TW_SMEM ? TWN_RAW : 0;
     static constexpr size_t SMEM = sizeof(cplx_t<R>) * (size_t(TWN) + size_t(G) * LS);
-    // 128 threads per CTA and <= 128 registers per thread: 4 CTAs (16 warps) per SM when shared memory allows
-    static constexpr int MINB = SMEM <= 54 * 1024 ? 4 : (SMEM <= 72 * 1024 ? 3 : (SMEM <= 110 * 1024 ? 2 : 1));
+    // 128-thread CTAs: <= 128 registers (4 CTAs per SM) when shared memory allows; one-line CTAs
+    // of L >= 1024 keep their registers (the SM holds as many lines as its register file allows)
+    static constexpr int MINB = WIDE ? 1 : (SMEM <= 54 * 1024 ? 4 : (SMEM <= 72 * 1024 ? 3 : (SMEM <= 110 * 1024 ? 2 : 1)));
 };
 
 // Barrier over the threads of one line: a named barrier when a line spans whole warps,
@@ -131,7 +150,7 @@ template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile(
 
 template <typename R, typename V>
 __device__ __forceinline__ void accumulate_red(const RedDesc& rd, double* acc, V v, const V* partner, long long flat,
-                                               const int* shift, const long long* nmask) {
+                                               long long lflat, const int* shift, const long long* nmask) {
 #pragma unroll
     for (int k = 0; k < MAX_RED; ++k) {
         if (k >= rd.n) break;
@@ -147,10 +166,72 @@ __device__ __forceinline__ void accumulate_red(const RedDesc& rd, double* acc, V
             const int ax = rd.waxis[k];
             val *= rd.wtab[k][(flat >> shift[ax]) & nmask[ax]];
         } else if (wk == WK_GRID) {
-            val *= rd.wtab[k][flat];
+            val *= rd.wtab[k][lflat];
         }
         acc[k] += val;
     }
+}
+
+// Reductions over the E values a thread holds of one line (m = tid + u*T): accumulator-outer so that
+// each accumulator's weight loads are issued together; weights along the pass axis are read per
+// element, weights along other axes once per line, full-grid weights from the line-major table.
+template <typename R, int E, int T>
+__device__ __forceinline__ void accumulate_line(const RedDesc& rd, double* acc, const cplx_t<R>* v,
+                                                const cplx_t<R>* partner, long long base, int log2S, long long lbase,
+                                                int tid, int axis, const int* shift, const long long* nmask) {
+    double a2[E];
+#pragma unroll
+    for (int u = 0; u < E; ++u) a2[u] = double(v[u].x) * double(v[u].x) + double(v[u].y) * double(v[u].y);
+#pragma unroll
+    for (int k = 0; k < MAX_RED; ++k) {
+        if (k >= rd.n) break;
+        double sum = 0.0;
+        const int wk = rd.wkind[k];
+        const double* __restrict__ wt = rd.wtab[k];
+        if (rd.kind[k] == RK_ABS2) {
+            if (wk == WK_ONE) {
+#pragma unroll
+                for (int u = 0; u < E; ++u) sum += a2[u];
+            } else if (wk == WK_AXIS && rd.waxis[k] == axis) {
+#pragma unroll
+                for (int u = 0; u < E; ++u) sum += a2[u] * __ldg(wt + tid + u * T);
+            } else if (wk == WK_AXIS) {
+                const int ax = rd.waxis[k];
+                const double wl = __ldg(wt + ((base >> shift[ax]) & nmask[ax]));
+#pragma unroll
+                for (int u = 0; u < E; ++u) sum += a2[u];
+                sum *= wl;
+            } else {
+                double wv[E];
+#pragma unroll
+                for (int u = 0; u < E; ++u) wv[u] = __ldg(wt + lbase + tid + u * T);
+#pragma unroll
+                for (int u = 0; u < E; ++u) sum += a2[u] * wv[u];
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < E; ++u) {
+                const int m = tid + u * T;
+                const long long flat = base + ((long long)m << log2S);
+                const cplx_t<R> p = partner[flat];
+                double val = double(p.x) * double(v[u].x) + double(p.y) * double(v[u].y);
+                if (wk == WK_AXIS) val *= __ldg(wt + ((flat >> shift[rd.waxis[k]]) & nmask[rd.waxis[k]]));
+                else if (wk == WK_GRID) val *= __ldg(wt + lbase + m);
+                sum += val;
+            }
+        }
+        acc[k] += sum;
+    }
+}
+
+// Warm L2 with the line-major rows a pass will read later (a full-grid table), one 128-byte
+// line per request.
+template <int L, int T, typename X> __device__ __forceinline__ void prefetch_row_l2(const X* row, int tid) {
+    constexpr int BYTES = L * int(sizeof(X));
+    constexpr int NLINES = (BYTES + 127) / 128;
+    const char* p = reinterpret_cast<const char*>(row);
+#pragma unroll
+    for (int q = tid; q < NLINES; q += T) asm volatile("prefetch.global.L2 [%0];" ::"l"(p + 128 * q));
 }
 
 // Block reduction of acc[0..n) into partials, then the last CTA sums the partials in order.
@@ -195,12 +276,49 @@ __device__ __forceinline__ void finish_red(const RedDesc& rd, double* acc) {
     if (t == 0) *rd.counter = 0u;
 }
 
+// Point-wise r-space factors on the E values a thread holds of one line: a full-grid table
+// (line-major: entry lbase + m), per-axis complex factors (the pass axis per element, the other
+// axes once per line), per-axis real factors and a scalar.
+template <typename R, int E, int T>
+__device__ __forceinline__ void apply_factors(cplx_t<R>* v, int tid, long long base, long long lbase,
+                                              const R* __restrict__ tr, const cplx_t<R>* __restrict__ tc,
+                                              const cplx_t<R>* const* axc, const R* const* axr, int axis, int dim,
+                                              const int* shift, const long long* nmask, const double* scale_dev) {
+    using V = cplx_t<R>;
+    V lf = V{R(1), R(0)};
+    R lr = R(1);
+    bool use_lf = false, use_lr = false;
+    const V* __restrict__ pc = axc ? axc[axis] : nullptr;
+    const R* __restrict__ pr = axr ? axr[axis] : nullptr;
+#pragma unroll
+    for (int k = 0; k < MAX_DIM; ++k) {
+        if (k >= dim || k == axis) continue;
+        const long long ik = (base >> shift[k]) & nmask[k];
+        if (axc && axc[k]) { lf = cmul(lf, axc[k][ik]); use_lf = true; }
+        if (axr && axr[k]) { lr *= axr[k][ik]; use_lr = true; }
+    }
+    if (scale_dev) { lr *= R(*scale_dev); use_lr = true; }
+#pragma unroll
+    for (int u = 0; u < E; ++u) {
+        const int m = tid + u * T;
+        V x = v[u];
+        if (tr) x = cscale(x, tr[lbase + m]);
+        if (tc) x = cmul(x, tc[lbase + m]);
+        if (pc) x = cmul(x, __ldg(pc + m));
+        if (pr) x = cscale(x, __ldg(pr + m));
+        if (use_lf) x = cmul(x, lf);
+        if (use_lr) x = cscale(x, lr);
+        v[u] = x;
+    }
+}
+
 template <typename R, int L, bool STRIDED, int MODE>
 __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
     qnd_pass_kernel(const __grid_constant__ PassArgs<R> a) {
     using V = cplx_t<R>;
     using SH = PassShape<R, L>;
     constexpr int E = SH::E, T = SH::T, G = SH::G, NT = SH::NT, LS = SH::LS;
+    constexpr bool TWS = SH::TW_SMEM;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* tw_s = reinterpret_cast<V*>(smem_raw);   // [TWN] stage twiddles (when they fit)
     V* lines = tw_s + SH::TWN;                   // [G][LS]
@@ -219,14 +337,28 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
     const long long lam = g * G + w;
     const bool active = lam < nlines;
     const long long base = line_base(active ? lam : 0);
+    const long long lbase = (active ? lam : 0) * L;  // line-major table offset of this line
+
     const V* tw = a.tw;
-    if constexpr (SH::TW_SMEM) {
+    if constexpr (TWS) {
         for (int i = t; i < FFTPlan<L, E>::tw_size(); i += NT) tw_s[i] = a.tw[i];
         tw = tw_s;
     }
 
     pdl_wait();
     pdl_launch_dependents();
+
+    if constexpr (MODE == PM_DOUBLE || MODE == PM_SANDWICH) {
+        // tables needed after the first transforms: start their journey to L2 now
+        if (active) {
+            if (a.mid_cplx) prefetch_row_l2<L, T>(a.mid_cplx + lbase, tid);
+            if (a.mid_real) prefetch_row_l2<L, T>(a.mid_real + lbase, tid);
+            if (a.epi_cplx) prefetch_row_l2<L, T>(a.epi_cplx + lbase, tid);
+            if (a.epi_real) prefetch_row_l2<L, T>(a.epi_real + lbase, tid);
+            for (int k = 0; k < a.red.n; ++k)
+                if (a.red.wkind[k] == WK_GRID) prefetch_row_l2<L, T>(a.red.wtab[k] + lbase, tid);
+        }
+    }
 
     V v[E];
     if constexpr (STRIDED) {
@@ -246,40 +378,14 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
         const V* __restrict__ src = a.psi;
 #pragma unroll
         for (int u = 0; u < E; ++u) v[u] = active ? src[base + tid + u * T] : V{R(0), R(0)};
-        if constexpr (SH::TW_SMEM) __syncthreads();  // twiddles visible
+        if constexpr (TWS) __syncthreads();  // twiddles visible
     }
 
-    if constexpr (MODE == PM_SANDWICH) {
-        if (active && (a.pro_real || a.pro_cplx || a.pro_scale_dev || a.ax_in_prologue)) {
-            const R sc = a.pro_scale_dev ? R(*a.pro_scale_dev) : R(1);
-            const R* __restrict__ pr = a.pro_real;
-            const V* __restrict__ pc = a.pro_cplx;
-            const V* __restrict__ axc = a.ax_in_prologue ? a.ax_cplx[a.axis] : nullptr;
-            V lf = V{R(1), R(0)};
-            R lr = R(1);
-            bool use_lf = false, use_lr = false;
-            if (a.ax_in_prologue) {
-#pragma unroll
-                for (int k = 0; k < MAX_DIM; ++k) {
-                    if (k >= a.dim || k == a.axis) continue;
-                    const long long ik = (base >> a.shift[k]) & a.nmask[k];
-                    if (a.ax_cplx[k]) { lf = cmul(lf, a.ax_cplx[k][ik]); use_lf = true; }
-                }
-            }
-            if (a.pro_scale_dev) { lr *= sc; use_lr = true; }
-#pragma unroll
-            for (int u = 0; u < E; ++u) {
-                const int m = tid + u * T;
-                const long long flat = base + ((long long)m << log2S);
-                V x = v[u];
-                if (pr) x = cscale(x, pr[flat]);
-                if (pc) x = cmul(x, pc[flat]);
-                if (axc) x = cmul(x, __ldg(axc + m));
-                if (use_lf) x = cmul(x, lf);
-                if (use_lr) x = cscale(x, lr);
-                v[u] = x;
-            }
-        }
+    constexpr bool PROPAGATE = MODE == PM_SANDWICH || MODE == PM_DOUBLE;
+    if constexpr (PROPAGATE) {
+        if (active && (a.pro_real || a.pro_cplx || a.pro_scale_dev || a.ax_in_prologue))
+            apply_factors<R, E, T>(v, tid, base, lbase, a.pro_real, a.pro_cplx, a.ax_in_prologue ? a.ax_cplx : nullptr,
+                                   nullptr, a.axis, a.dim, a.shift, a.nmask, a.pro_scale_dev);
     }
     if constexpr (STRIDED) lsync();  // staged inputs read before the exchanges reuse the buffer
 
@@ -288,9 +394,9 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
     for (int k = 0; k < MAX_RED; ++k) acc[k] = 0.0;
 
     if constexpr (MODE == PM_FFT_INV) {
-        fft_line_stages<L, E, +1, 0, SH::TW_SMEM>(v, tid, line, tw, lsync);
+        fft_line_stages<L, E, +1, 0, TWS>(v, tid, line, tw, lsync);
     } else {
-        fft_line_stages<L, E, -1, 0, SH::TW_SMEM>(v, tid, line, tw, lsync);
+        fft_line_stages<L, E, -1, 0, TWS>(v, tid, line, tw, lsync);
     }
 
     bool store_out = false;  // write v back to psi at the end
@@ -299,57 +405,39 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
         for (int u = 0; u < E; ++u) v[u] = cscale(v[u], a.scale);
         store_out = true;
     } else if constexpr (MODE == PM_SPECRED) {
-        if (active) {
-#pragma unroll
-            for (int u = 0; u < E; ++u) {
-                const long long flat = base + ((long long)(tid + u * T) << log2S);
-                accumulate_red<R>(a.red, acc, v[u], a.partner, flat, a.shift, a.nmask);
-            }
-        }
+        if (active) accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);
     } else {
-        // SANDWICH and APPLY: spectral multiply, inverse transform
+        // SANDWICH / DOUBLE / APPLY: spectral multiply, inverse transform
         if (a.spec) {
             const V* __restrict__ sp = a.spec;
 #pragma unroll
             for (int u = 0; u < E; ++u) v[u] = cmul(v[u], __ldg(sp + tid + u * T));
         }
-        fft_line_stages<L, E, +1, 0, SH::TW_SMEM>(v, tid, line, tw, lsync);
+        fft_line_stages<L, E, +1, 0, TWS>(v, tid, line, tw, lsync);
+        if constexpr (MODE == PM_DOUBLE) {
+            // r-space factor between the two sandwiches, then the second sandwich on the same axis
+            if (active)
+                apply_factors<R, E, T>(v, tid, base, lbase, a.mid_real, a.mid_cplx, a.mid_ax_cplx, nullptr, a.axis,
+                                       a.dim, a.shift, a.nmask, nullptr);
+            fft_line_stages<L, E, -1, 0, TWS>(v, tid, line, tw, lsync);
+            if (a.spec2) {
+                const V* __restrict__ sp2 = a.spec2;
+#pragma unroll
+                for (int u = 0; u < E; ++u) v[u] = cmul(v[u], __ldg(sp2 + tid + u * T));
+            }
+            fft_line_stages<L, E, +1, 0, TWS>(v, tid, line, tw, lsync);
+        }
         if (active) {
-            if constexpr (MODE == PM_SANDWICH) {
-                const R* __restrict__ er = a.epi_real;
-                const V* __restrict__ ec = a.epi_cplx;
-                const V* __restrict__ axc = a.ax_in_prologue ? nullptr : a.ax_cplx[a.axis];
-                const R* __restrict__ axr = a.ax_real[a.axis];
-                V lf = V{R(1), R(0)};
-                R lr = R(1);
-                bool use_lf = false, use_lr = false;
-#pragma unroll
-                for (int k = 0; k < MAX_DIM; ++k) {
-                    if (k >= a.dim || k == a.axis) continue;
-                    const long long ik = (base >> a.shift[k]) & a.nmask[k];
-                    if (a.ax_cplx[k] && !a.ax_in_prologue) { lf = cmul(lf, a.ax_cplx[k][ik]); use_lf = true; }
-                    if (a.ax_real[k]) { lr *= a.ax_real[k][ik]; use_lr = true; }
-                }
-#pragma unroll
-                for (int u = 0; u < E; ++u) {
-                    const int m = tid + u * T;
-                    const long long flat = base + ((long long)m << log2S);
-                    V x = v[u];
-                    if (er) x = cscale(x, er[flat]);
-                    if (ec) x = cmul(x, ec[flat]);
-                    if (axc) x = cmul(x, __ldg(axc + m));
-                    if (axr) x = cscale(x, __ldg(axr + m));
-                    if (use_lf) x = cmul(x, lf);
-                    if (use_lr) x = cscale(x, lr);
-                    v[u] = x;
-                }
-                if (a.red.n) {
-#pragma unroll
-                    for (int u = 0; u < E; ++u) {
-                        const long long flat = base + ((long long)(tid + u * T) << log2S);
-                        accumulate_red<R>(a.red, acc, v[u], a.partner, flat, a.shift, a.nmask);
-                    }
-                }
+            if constexpr (PROPAGATE) {
+                if (a.epi_real || a.epi_cplx || !a.ax_in_prologue)
+                    apply_factors<R, E, T>(v, tid, base, lbase, a.epi_real, a.epi_cplx,
+                                           a.ax_in_prologue ? nullptr : a.ax_cplx, a.ax_real, a.axis, a.dim, a.shift,
+                                           a.nmask, nullptr);
+                else
+                    apply_factors<R, E, T>(v, tid, base, lbase, nullptr, nullptr, nullptr, a.ax_real, a.axis, a.dim,
+                                           a.shift, a.nmask, nullptr);
+                if (a.red.n)
+                    accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);
             } else {  // PM_APPLY
 #pragma unroll
                 for (int u = 0; u < E; ++u) {
@@ -363,20 +451,15 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
                     if (a.apply_acc) x = cadd(x, a.dst[flat]);
                     v[u] = x;
                 }
-                if (a.red.n) {
-#pragma unroll
-                    for (int u = 0; u < E; ++u) {
-                        const long long flat = base + ((long long)(tid + u * T) << log2S);
-                        accumulate_red<R>(a.red, acc, v[u], a.partner, flat, a.shift, a.nmask);
-                    }
-                }
+                if (a.red.n)
+                    accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);
                 if (a.dst) {
 #pragma unroll
                     for (int u = 0; u < E; ++u) a.dst[base + ((long long)(tid + u * T) << log2S)] = v[u];
                 }
             }
         }
-        store_out = MODE == PM_SANDWICH;
+        store_out = PROPAGATE;
     }
 
     if (store_out) {
@@ -410,7 +493,7 @@ __global__ void __launch_bounds__(256) qnd_grid_reduce_kernel(const __grid_const
 #pragma unroll
     for (int k = 0; k < MAX_RED; ++k) acc[k] = 0.0;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        accumulate_red<R>(a.red, acc, a.psi[i], a.partner, i, a.shift, a.nmask);
+        accumulate_red<R>(a.red, acc, a.psi[i], a.partner, i, i, a.shift, a.nmask);
     finish_red<256>(a.red, acc);
 }
 

@@ -19,6 +19,7 @@ template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int m
     case PM_FFT_INV: fn = QND_PICK(PM_FFT_INV); break;
     case PM_SPECRED: fn = QND_PICK(PM_SPECRED); break;
     case PM_APPLY: fn = QND_PICK(PM_APPLY); break;
+    case PM_DOUBLE: fn = QND_PICK(PM_DOUBLE); break;
     default: fn = nullptr;
     }
 #undef QND_PICK
