@@ -130,6 +130,22 @@ int qnd_observables(qnd_ctx *ctx, const void *psi_r_dev, int nobs, const char *c
 /* Calculation_global_energies (calculate_observables.c:89-116): out[m] = Re <psi|H^(m+1)|psi> dNr. */
 int qnd_energies(qnd_ctx *ctx, const void *psi_r_dev, int n, double *out_host);
 
+/* ---- r-space observables without allocation (no reference counterpart).
+ * Computes the "norm", "dipole_r" and "accel" values of qnd_observables, in the same row layout,
+ * with the same reduction, into the caller's device buffer out_dev[nvalues]. It is asynchronous
+ * on the context's stream.
+ * It allocates no memory, for callers that must not call cudaMalloc/cudaFree: a monitor sampling
+ * a state between the steps of a device-resident loop (cudaFree synchronises the whole device),
+ * or a process whose device memory is already reserved by another allocator's pool.
+ * Scratch: a fixed 38,144-byte device array per device (partial sums of up to 592 CTAs + a ticket
+ * counter that must be zero at launch; the kernel leaves it zero).
+ * The first call on a device does a one-time set-up that synchronises the stream; make it before
+ * any stream capture. Concurrent calls on one device share the scratch and race: serialise them.
+ * Limits: at most 64 values per call (QND_EINVAL beyond). "dipole_v", "energy" and "Lz" give
+ * QND_EUNSUPPORTED. "accel" needs qnd_set_gradv for every axis. */
+int qnd_observables_rspace_noalloc(qnd_ctx *ctx, const void *psi_r_dev, int nobs, const char *const *names,
+                                   double *out_dev);
+
 #ifdef __cplusplus
 }
 #endif

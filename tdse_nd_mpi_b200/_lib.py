@@ -53,6 +53,7 @@ SIGNATURES = {
     "qnd_observable_count": ([_vp, C.c_int, _names, _ip], C.c_int),
     "qnd_observables": ([_vp, _vp, C.c_int, _names, _dp, _dp], C.c_int),
     "qnd_energies": ([_vp, _vp, C.c_int, _dp], C.c_int),
+    "qnd_observables_rspace_noalloc": ([_vp, _vp, C.c_int, _names, _vp], C.c_int),
 }
 
 _lib = None

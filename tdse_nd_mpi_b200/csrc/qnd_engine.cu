@@ -22,6 +22,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -1678,3 +1679,154 @@ int qnd_energies(qnd_ctx* ctx, const void* psi_r_dev, int n, double* out_host) {
 }
 
 }  // extern "C"
+
+// ============================================== r-space observables, no allocation ==
+//
+// qnd_observables_rspace_noalloc evaluates the r-space observables of qnd_observables
+// ("norm", "dipole_r", "accel") with the same grid-reduction kernel and the same CTA count,
+// so it adds the same partial sums in the same order. It differs in three ways:
+//  - the reduction scratch is a fixed device array in this file, not the context's
+//    growable buffers;
+//  - the values go to a caller device buffer, not through a host copy;
+//  - it allocates no device, pinned or host memory and does not synchronise.
+//
+// It serves callers that must not call cudaMalloc or cudaFree:
+//  - A monitor that samples a state between the steps of a device-resident loop. Growing a
+//    buffer frees the old one, and cudaFree synchronises the whole device, stalling the
+//    propagation and every other stream.
+//  - A process whose device memory is already reserved by another allocator's pool. There a
+//    new cudaMalloc fails.
+//
+// The first call on a device does a one-time set-up with that device current: it resolves
+// the scratch array's address and zeroes its ticket counter, which synchronises the context's
+// stream once. Make that first call before any stream capture.
+//
+// All calls on one device share the one scratch array. Calls whose launches can overlap
+// (different streams without ordering between them) race on it and give wrong sums.
+// Serialise them.
+
+namespace qnd {
+
+constexpr int NOALLOC_MAX_BLOCKS = 148 * 4;   // CTAs of one grid reduction (the cap of reduce_blocks)
+constexpr int NOALLOC_MAX_VALUES = 64;        // observable values per call
+constexpr size_t NOALLOC_PARTIALS = size_t(NOALLOC_MAX_BLOCKS) * MAX_RED;  // doubles
+constexpr size_t NOALLOC_COUNTER_SLOT = 32;   // doubles (256 bytes) holding the ticket counter word
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+// Reduction scratch: [NOALLOC_MAX_BLOCKS][MAX_RED] partial sums (37,888 bytes), then the
+// ticket counter (one 32-bit word in a 256-byte slot): 38,144 bytes per device.
+//  - The counter word must be zero when a reduction starts. Static device storage is zero at
+//    module load, the set-up zeroes it again, and the last CTA of every reduction resets it.
+//  - The partial sums need no initial value: each CTA writes its own slot before it takes a
+//    ticket.
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_PARTIALS + NOALLOC_COUNTER_SLOT];
+
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[NOALLOC_MAX_DEVICES];  // per device, filled by the set-up
+
+// Address of this device's scratch array; the set-up runs once per device, c->device current.
+static double* noalloc_scratch(qnd_ctx* c) {
+    if (c->device < 0 || c->device >= NOALLOC_MAX_DEVICES)
+        QND_FAIL(QND_EUNSUPPORTED, "qnd_observables_rspace_noalloc: device %d is beyond the %d devices it tracks",
+                 c->device, NOALLOC_MAX_DEVICES);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    double*& p = g_noalloc_ptr[c->device];
+    if (!p) {
+        void* q = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&q, g_noalloc_scratch);
+        if (e != cudaSuccess || !q) {
+            cudaGetLastError();
+            QND_FAIL(QND_ECUDA, "qnd_observables_rspace_noalloc: cudaGetSymbolAddress of the scratch array on device %d: %s",
+                     c->device, cudaGetErrorString(e));
+        }
+        double* base = static_cast<double*>(q);
+        QND_CK(cudaMemsetAsync(base + NOALLOC_PARTIALS, 0, NOALLOC_COUNTER_SLOT * sizeof(double), c->stream));
+        QND_CK(cudaStreamSynchronize(c->stream));
+        p = base;
+    }
+    return p;
+}
+
+template <typename R>
+static void noalloc_launch(qnd_ctx* c, const void* psi, const RedDesc& rd, double* scratch, int nblocks) {
+    PassSpec ps;
+    ps.psi = const_cast<void*>(psi);
+    ps.red = rd;
+    PassArgs<R> a;
+    fill_args<R>(c, ps, a);
+    a.red.partials = scratch;
+    a.red.counter = reinterpret_cast<unsigned int*>(scratch + NOALLOC_PARTIALS);
+    launch_grid_reduce<R>(a, c->n, c->stream, nblocks);
+    c->kernels_launched++;
+    QND_CK(cudaGetLastError());
+}
+
+}  // namespace qnd
+
+extern "C" int qnd_observables_rspace_noalloc(qnd_ctx* ctx, const void* psi_r_dev, int nobs, const char* const* names,
+                                              double* out_dev) {
+    using namespace qnd;
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_r_dev);
+    if (nobs < 0) QND_FAIL(QND_EINVAL, "qnd_observables_rspace_noalloc: nobs = %d", nobs);
+    if (nobs > 0) QND_NEED(names);
+    // Values per name, in qnd_observables' row layout; the k-space observables need transform
+    // passes whose tables and scratch states the context allocates on first use.
+    int nv = 0;
+    for (int k = 0; k < nobs; ++k) {
+        const char* nm = names[k] ? names[k] : "";
+        if (!strcmp(nm, "norm")) nv += 1;
+        else if (!strcmp(nm, "dipole_r")) nv += ctx->dim;
+        else if (!strcmp(nm, "accel")) {
+            for (int j = 0; j < ctx->dim; ++j)
+                if (!ctx->gradv_dev[j].p) QND_FAIL(QND_EINVAL, "observable 'accel' needs qnd_set_gradv for every axis");
+            nv += ctx->dim;
+        } else if (!strcmp(nm, "dipole_v") || !strcmp(nm, "energy") || !strcmp(nm, "Lz"))
+            QND_FAIL(QND_EUNSUPPORTED,
+                     "qnd_observables_rspace_noalloc: '%s' needs k-space passes; only norm, dipole_r and accel are "
+                     "evaluated without allocation (use qnd_observables)", nm);
+    }
+    if (nv > NOALLOC_MAX_VALUES)
+        QND_FAIL(QND_EINVAL, "qnd_observables_rspace_noalloc: %d observable values requested, at most %d per call", nv,
+                 NOALLOC_MAX_VALUES);
+    if (nv == 0) return QND_OK;
+    QND_NEED(out_dev);
+    const int nblocks = reduce_blocks(ctx);
+    if (nblocks > NOALLOC_MAX_BLOCKS)
+        QND_FAIL(QND_EUNSUPPORTED,
+                 "qnd_observables_rspace_noalloc: the reduction needs %d CTAs x %d partial sums of scratch, the static "
+                 "array holds %d CTAs", nblocks, MAX_RED, NOALLOC_MAX_BLOCKS);
+    set_device(ctx);
+    double* scratch = noalloc_scratch(ctx);
+    // Contiguous runs of at most MAX_RED values per launch, in row order.
+    RedDesc cur{};
+    int off = 0;
+    auto flush = [&]() {
+        if (!cur.n) return;
+        if (ctx->fp64) noalloc_launch<double>(ctx, psi_r_dev, cur, scratch, nblocks);
+        else noalloc_launch<float>(ctx, psi_r_dev, cur, scratch, nblocks);
+        cur = RedDesc{};
+    };
+    auto add = [&](int wkind, int waxis, const double* wtab, double scale) {
+        if (cur.n == MAX_RED) flush();
+        if (!cur.n) cur.out = out_dev + off;
+        cur.kind[cur.n] = RK_ABS2;
+        cur.wkind[cur.n] = wkind;
+        cur.waxis[cur.n] = waxis;
+        cur.wtab[cur.n] = wtab;
+        cur.scale[cur.n] = scale;
+        cur.n++;
+        off++;
+    };
+    for (int k = 0; k < nobs; ++k) {
+        const char* nm = names[k] ? names[k] : "";
+        if (!strcmp(nm, "norm")) add(WK_ONE, 0, nullptr, ctx->dNr);
+        else if (!strcmp(nm, "dipole_r"))
+            for (int j = 0; j < ctx->dim; ++j) add(WK_AXIS, j, ctx->r_dev.as<double>() + ctx->axoff[j], ctx->dNr);
+        else if (!strcmp(nm, "accel"))
+            for (int j = 0; j < ctx->dim; ++j) add(WK_GRID, 0, ctx->gradv_dev[j].as<double>(), -ctx->dNr);
+    }
+    flush();
+    QND_API_END
+}
