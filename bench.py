@@ -9,8 +9,11 @@ Workload (one "step" = one BM4 time step with its observables):
   only (no dataset).
 
 Reported (one JSON line on rank 0):
-  value      device-resident steps/s over all ranks (inputs already in HBM, the L2 flushed
-             with a 256 MB write between timed steps, CUDA events per step, max over ranks)
+  value      device-resident steps/s over all ranks: inputs already in HBM, steps timed in calls
+             of 100 consecutive steps (one device-resident chain each, the state on chip between
+             steps as in a long propagation), a 256 MB write flushing the L2 before every call,
+             CUDA events per call, max over ranks
+  flush_every_step  the same with one call per step and the L2 flushed before every step
   e2e        the same steps through the public C ABI with pinned host buffers: state upload,
              qnd_run_length (field H2D and observable D2H every step), state download
   roofline   the fused axis-pass kernel: algorithmic bytes per launch / its mean event time
@@ -286,19 +289,31 @@ def ground_state(torch, V, stream, nsteps):
     return psi
 
 
-def timed_steps(torch, grid, psi_t, E_dev, obs_dev, names, i0, steps, warmup, flush):
-    """Warm-up, then `steps` single-step calls each bracketed by CUDA events, the L2 flushed between."""
-    for k in range(warmup):
+BLOCK = 100  # consecutive steps per timed call (one device-resident chain); the L2 is flushed between calls
+
+
+def timed_steps(torch, grid, psi_t, E_dev, obs_dev, names, i0, steps, warmup, flush, block=BLOCK):
+    """Warm-up, then `steps` steps as calls of `block` consecutive steps (the last one shorter), each
+    call bracketed by CUDA events and preceded by an untimed 256 MB write that flushes the L2. Within a
+    call the state stays on chip between steps, as in a long propagation."""
+    def calls(n, first):
+        k = 0
+        while k < n:
+            b = min(block, n - k)
+            yield first + k, b
+            k += b
+    for k, b in calls(warmup, 0):
         flush.zero_()
-        grid.run_length_dev(psi_t, E_dev[i0 + k], 1, names, obs_dev[k])
+        grid.run_length_dev(psi_t, E_dev[i0 + k:i0 + k + b], b, names, obs_dev[k:k + b])
     torch.cuda.synchronize()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
-    for k in range(steps):
+    todo = list(calls(steps, warmup))
+    starts = [torch.cuda.Event(enable_timing=True) for _ in todo]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in todo]
+    for (k, b), st, en in zip(todo, starts, ends):
         flush.zero_()
-        starts[k].record()
-        grid.run_length_dev(psi_t, E_dev[i0 + warmup + k], 1, names, obs_dev[warmup + k])
-        ends[k].record()
+        st.record()
+        grid.run_length_dev(psi_t, E_dev[i0 + k:i0 + k + b], b, names, obs_dev[k:k + b])
+        en.record()
     torch.cuda.synchronize()
     return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
 
@@ -372,6 +387,12 @@ def main():
     timed_steps(torch, grid, psi_t2, E_dev, obs_dev, OBS, i0, prof_steps, 0, flush)
     _, passes, pass_ms = grid.get_profile(reset=True)
     grid.set_profiling(False)
+    # the same steps one call per step with the L2 flushed before each (no on-chip state across steps)
+    fs_steps = min(args.steps, 100)
+    psi_t3 = torch.tensor(psi0.view(np.float64), device=dev).contiguous()
+    ms_fs = timed_steps(torch, grid, psi_t3, E_dev, obs_dev, OBS, i0, fs_steps, 0, flush, block=1) / fs_steps
+    flush_every_step = {"value": 1000.0 / ms_fs, "unit": "steps/s", "ms_per_step": ms_fs, "steps": fs_steps,
+                        "what": "rank-local: one qnd_run_length_dev call per step, 256 MB L2 flush before each step"}
     n = NR * NR
     # Algorithmic bytes (the survey's accounting): every full-grid N-D transform is one read and one
     # write of the state, 2*N*16 bytes; a BM4 length-gauge step is 2s = 12 transforms plus the 2 of
@@ -470,8 +491,9 @@ def main():
         "config": {"workload": "H_2D 1024x1024 real-time BM4 length gauge, dt=0.05, 800nm 1e14 W/cm^2 8-cycle "
                                "sin^2, cos^(1/8) mask, norm+dipole+accel every step",
                    "nr": [NR, NR], "dr": DR, "dt": DT, "integrator": INTEG, "parallelism": f"replicas x{world}",
-                   "l2": "state 16.8 MB < L2; 256 MB L2 flush between timed steps"},
+                   "l2": f"state 16.8 MB < L2; timed in calls of {BLOCK} consecutive steps with a 256 MB L2 flush before each call"},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": gpu_launches,
+        "flush_every_step": flush_every_step,
         "clocks": clk.summary(),
     }
     line.update(extras)

@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -368,6 +369,8 @@ struct PassSpec {
     const void* mid_real = nullptr;
     const void* mid_cplx = nullptr;
     const void* mid_ax_cplx[MAX_DIM] = {nullptr, nullptr, nullptr};
+    const void* mid_ax_real[MAX_DIM] = {nullptr, nullptr, nullptr};
+    int red_at_mid = 0;
     const void* epi_real = nullptr;
     const void* epi_cplx = nullptr;
     const void* ax_cplx[MAX_DIM] = {nullptr, nullptr, nullptr};
@@ -407,7 +410,11 @@ template <typename R> static void fill_args(qnd_ctx* c, const PassSpec& ps, Pass
     a.spec2 = static_cast<const V*>(ps.spec2);
     a.mid_real = static_cast<const R*>(ps.mid_real);
     a.mid_cplx = static_cast<const V*>(ps.mid_cplx);
-    for (int k = 0; k < MAX_DIM; ++k) a.mid_ax_cplx[k] = static_cast<const V*>(ps.mid_ax_cplx[k]);
+    for (int k = 0; k < MAX_DIM; ++k) {
+        a.mid_ax_cplx[k] = static_cast<const V*>(ps.mid_ax_cplx[k]);
+        a.mid_ax_real[k] = static_cast<const R*>(ps.mid_ax_real[k]);
+    }
+    a.red_at_mid = ps.red_at_mid;
     a.epi_real = static_cast<const R*>(ps.epi_real);
     a.epi_cplx = static_cast<const V*>(ps.epi_cplx);
     for (int k = 0; k < MAX_DIM; ++k) {
@@ -779,18 +786,31 @@ static bool has_mask(const qnd_ctx* c) {
 }
 
 // ---------------------------------------------------------------- sandwich chains --
-//
-// A split-operator step is a chain of kinetic sandwiches K_0 .. K_{NK-1} (each a product of one
-// pass per axis) with point-wise r-space factors M_i between K_i and K_{i+1}, an optional factor
-// before K_0 and one after K_{NK-1}. Consecutive sandwiches run their axes in opposite orders, so
-// the last axis of K_i is the first axis of K_{i+1}: those two axis passes and M_i fuse into one
-// PM_DOUBLE pass. A 2-D step costs NK + 1 passes instead of 2 NK; a 3-D step 2 NK + 1 instead of
-// 3 NK; in 1-D the sandwiches pair up two per pass.
 
 struct Factor {
     int kind = -1;        // RT_IMAG (real table), RT_LENGTH / RT_VEL (complex), -1: none
     double a = 0.0, b = NO_COEF;
     int laser_ia = -1;    // length gauge: per-axis laser phases of sub-step laser_ia
+};
+
+// A kinetic sandwich: exp(-i coef p_j^2/2)/N_j (SP_LENGTH), exp(-coef p_j^2/2)/N_j (SP_IMAG), or
+// the velocity-gauge k-space phases of sub-step ia of chunk step lst (KV_FIELD).
+constexpr int KV_FIELD = 100;
+struct ChainK {
+    int kind = SP_LENGTH;
+    double coef = 0.0;
+    int64_t lst = 0;
+    int ia = 0;
+};
+
+// Point-wise r-space work between two sandwiches (or after the last one): a factor (a full-grid
+// table and/or the laser phases of chunk step lst), the step mask, then reductions of the state.
+struct ChainMid {
+    Factor f;
+    int64_t lst = 0;
+    bool mask = false;
+    const RedDesc* red = nullptr;
+    bool empty() const { return f.kind < 0 && f.laser_ia < 0 && !mask && !red; }
 };
 
 static void set_factor(qnd_ctx* c, const Factor& f, int ax, int64_t lst, const void** treal, const void** tcplx,
@@ -804,38 +824,61 @@ static void set_factor(qnd_ctx* c, const Factor& f, int ax, int64_t lst, const v
         for (int j = 0; j < c->dim; ++j) axc[j] = field_slice(c, lst, f.laser_ia, j);
 }
 
-// Axis of the chain's last pass (the one that carries the final factor, mask and reductions).
-static int chain_final_axis(const qnd_ctx* c, int NK) {
-    if (c->dim == 1) return 0;
-    return ((NK - 1) % 2 == 0) ? 0 : c->dim - 1;
+static const void* chain_spec(qnd_ctx* c, const ChainK& k, int ax) {
+    if (k.kind == KV_FIELD) return field_slice(c, k.lst, k.ia, ax);
+    return spec_table(c, k.kind, ax, k.coef);
 }
 
-template <class SpecFn, class MidFn>
-static void sandwich_chain(qnd_ctx* c, void* psi, int NK, SpecFn spec_of, MidFn mid_of, const Factor& pre,
-                           const double* pre_scale, const Factor& post, bool masked, const RedDesc* fin,
-                           int64_t lst) {
+// Axis of the pass that ends sandwich i of a chain (it carries the factor after sandwich i).
+static int sandwich_last_axis(const qnd_ctx* c, int64_t i) {
+    if (c->dim == 1) return 0;
+    return (i % 2 == 0) ? 0 : c->dim - 1;
+}
+
+// Axis of the chain's last pass (the one that carries the final factor, mask and reductions).
+static int chain_final_axis(const qnd_ctx* c, int NK) { return sandwich_last_axis(c, NK - 1); }
+
+// Run a chain of kinetic sandwiches K_0 .. K_{NK-1} with M[i] between K_i and K_{i+1}, `pre` (and
+// the device scalar pre_scale) before K_0 and `post` after K_{NK-1}. Consecutive sandwiches run
+// their axes in opposite orders, so the last axis of K_i is the first axis of K_{i+1}: those two
+// axis passes and M[i] fuse into one PM_DOUBLE pass. A chain of NK sandwiches costs NK + 1 passes
+// in 2-D (2 NK + 1 in 3-D) instead of d NK; in 1-D the sandwiches pair up two per pass, and a
+// factor between pairs moves into the next pass's prologue (1-D chains carry no mask or
+// reductions between sandwiches).
+static void run_chain(qnd_ctx* c, void* psi, const std::vector<ChainK>& K, const std::vector<ChainMid>& M,
+                      const Factor& pre, int64_t pre_lst, const double* pre_scale, const ChainMid& post) {
     const int d = c->dim;
+    const int64_t NK = int64_t(K.size());
+    if (NK == 0 || int64_t(M.size()) != NK - 1) QND_FAIL(QND_EINVAL, "internal: malformed sandwich chain");
     auto finish = [&](PassSpec& ps) {
-        set_factor(c, post, ps.axis, lst, &ps.epi_real, &ps.epi_cplx, nullptr);
-        if (masked)
+        set_factor(c, post.f, ps.axis, post.lst, &ps.epi_real, &ps.epi_cplx, nullptr);
+        if (post.mask)
             for (int j = 0; j < d; ++j) ps.ax_real[j] = c->mask_dev[j].p;
-        if (fin) ps.red = *fin;
+        if (post.red) ps.red = *post.red;
     };
     if (d == 1) {
-        int i = 0;
+        int64_t i = 0;
         while (i < NK) {
             PassSpec ps;
             ps.axis = 0;
             ps.psi = psi;
-            ps.spec = spec_of(i, 0);
-            const Factor before = i == 0 ? pre : mid_of(i - 1);
-            set_factor(c, before, 0, lst, &ps.pro_real, &ps.pro_cplx, ps.ax_cplx);
-            if (before.laser_ia >= 0) ps.ax_in_prologue = 1;
-            if (i == 0) ps.pro_scale = pre_scale;
+            ps.spec = chain_spec(c, K[i], 0);
+            if (i == 0) {
+                set_factor(c, pre, 0, pre_lst, &ps.pro_real, &ps.pro_cplx, ps.ax_cplx);
+                if (pre.laser_ia >= 0) ps.ax_in_prologue = 1;
+                ps.pro_scale = pre_scale;
+            } else {
+                const ChainMid& b = M[i - 1];
+                if (b.mask || b.red) QND_FAIL(QND_EINVAL, "internal: 1-D chain with a mask or reduction inside");
+                set_factor(c, b.f, 0, b.lst, &ps.pro_real, &ps.pro_cplx, ps.ax_cplx);
+                if (b.f.laser_ia >= 0) ps.ax_in_prologue = 1;
+            }
             if (i + 1 < NK) {
+                const ChainMid& m = M[i];
+                if (m.mask || m.red) QND_FAIL(QND_EINVAL, "internal: 1-D chain with a mask or reduction inside");
                 ps.mode = PM_DOUBLE;
-                set_factor(c, mid_of(i), 0, lst, &ps.mid_real, &ps.mid_cplx, ps.mid_ax_cplx);
-                ps.spec2 = spec_of(i + 1, 0);
+                set_factor(c, m.f, 0, m.lst, &ps.mid_real, &ps.mid_cplx, ps.mid_ax_cplx);
+                ps.spec2 = chain_spec(c, K[i + 1], 0);
                 i += 2;
             } else {
                 i += 1;
@@ -845,22 +888,29 @@ static void sandwich_chain(qnd_ctx* c, void* psi, int NK, SpecFn spec_of, MidFn 
         }
         return;
     }
-    for (int i = 0; i < NK; ++i) {
+    for (int64_t i = 0; i < NK; ++i) {
         for (int q = (i > 0 ? 1 : 0); q < d; ++q) {
             const int ax = (i % 2 == 0) ? d - 1 - q : q;
             PassSpec ps;
             ps.axis = ax;
             ps.psi = psi;
-            ps.spec = spec_of(i, ax);
+            ps.spec = chain_spec(c, K[i], ax);
             if (i == 0 && q == 0) {
-                set_factor(c, pre, ax, lst, &ps.pro_real, &ps.pro_cplx, ps.ax_cplx);
+                set_factor(c, pre, ax, pre_lst, &ps.pro_real, &ps.pro_cplx, ps.ax_cplx);
                 if (pre.laser_ia >= 0) ps.ax_in_prologue = 1;
                 ps.pro_scale = pre_scale;
             }
             if (q == d - 1 && i + 1 < NK) {
+                const ChainMid& m = M[i];
                 ps.mode = PM_DOUBLE;
-                set_factor(c, mid_of(i), ax, lst, &ps.mid_real, &ps.mid_cplx, ps.mid_ax_cplx);
-                ps.spec2 = spec_of(i + 1, ax);
+                set_factor(c, m.f, ax, m.lst, &ps.mid_real, &ps.mid_cplx, ps.mid_ax_cplx);
+                if (m.mask)
+                    for (int j = 0; j < d; ++j) ps.mid_ax_real[j] = c->mask_dev[j].p;
+                if (m.red) {
+                    ps.red = *m.red;
+                    ps.red_at_mid = 1;
+                }
+                ps.spec2 = chain_spec(c, K[i + 1], ax);
             }
             if (q == d - 1 && i + 1 == NK) finish(ps);
             launch_pass(c, ps);
@@ -868,63 +918,137 @@ static void sandwich_chain(qnd_ctx* c, void* psi, int NK, SpecFn spec_of, MidFn 
     }
 }
 
-// Integration_step_imag x nsteps on an r-space psi (integrators.c:135-163): V(a_0) K(h_0) V(a_1)V(a_2)
-// K(h_1) ... K(h_{s-1}) V(a_{2s-1}). pro_scale (device scalar, may be null) multiplies psi before the
-// first step (the deferred Gram-Schmidt normalisation).
+// Reductions after step k of a multi-step chain, with full-grid weights laid out line-major for
+// pass axis `axis` (the pass that carries them); at most one descriptor.
+using RedFn = std::function<std::vector<RedDesc>(int64_t k, int axis)>;
+
+// Integration_step_imag x nsteps on an r-space psi (integrators.c:135-163): per step V(a_0) K(h_0)
+// V(a_1)V(a_2) K(h_1) ... K(h_{s-1}) V(a_{2s-1}); between steps V(a_{2s-1})V(a_0) is one factor.
+// pro_scale (device scalar, may be null) multiplies psi first (the deferred Gram-Schmidt
+// normalisation).
 static void imag_steps(qnd_ctx* c, void* psi, int64_t nsteps, const double* pro_scale) {
     check_imag_clamp(c);
-    for (int64_t st = 0; st < nsteps; ++st) {
-        auto spec_of = [&](int i, int ax) { return spec_table(c, SP_IMAG, ax, c->as[2 * i] + c->as[2 * i + 1]); };
-        auto mid_of = [&](int i) {
-            Factor f;
-            f.kind = RT_IMAG;
-            f.a = c->as[2 * i + 1];
-            f.b = c->as[2 * i + 2];
-            return f;
-        };
-        Factor pre, post;
-        pre.kind = post.kind = RT_IMAG;
-        pre.a = c->as[0];
-        post.a = c->as[2 * c->s - 1];
-        sandwich_chain(c, psi, c->s, spec_of, mid_of, pre, st == 0 ? pro_scale : nullptr, post, false, nullptr, 0);
-    }
+    if (nsteps <= 0) return;
+    const int s = c->s;
+    std::vector<ChainK> K;
+    std::vector<ChainMid> M;
+    for (int64_t st = 0; st < nsteps; ++st)
+        for (int i = 0; i < s; ++i) {
+            if (i > 0 || st > 0) {
+                ChainMid m;
+                m.f.kind = RT_IMAG;
+                m.f.a = i > 0 ? c->as[2 * i - 1] : c->as[2 * s - 1];
+                m.f.b = c->as[2 * i];
+                M.push_back(m);
+            }
+            ChainK k;
+            k.kind = SP_IMAG;
+            k.coef = c->as[2 * i] + c->as[2 * i + 1];
+            K.push_back(k);
+        }
+    Factor pre;
+    ChainMid post;
+    pre.kind = post.f.kind = RT_IMAG;
+    pre.a = c->as[0];
+    post.f.a = c->as[2 * s - 1];
+    run_chain(c, psi, K, M, pre, 0, pro_scale, post);
 }
 
-// One length-gauge step in r-space (integrators.c:170-194 rewritten in r-space; chunk-local step
-// index lst for the field tables): K(a_0) V(h_0) K(a_1 + a_2) V(h_1) ... V(h_{s-1}) K(a_{2s-1}), then
-// the step mask and the fused reductions `fin` (of psi(t_{n+1})).
-static void length_step(qnd_ctx* c, void* psi, int64_t lst, const RedDesc* fin, bool masked) {
+// Length-gauge steps lst0 .. lst0+n-1 of the current field chunk in r-space (integrators.c:170-194
+// rewritten in r-space): per step K(a_0) V(h_0) K(a_1 + a_2) V(h_1) ... V(h_{s-1}) K(a_{2s-1}); after
+// each step the step mask and the reductions red_fn(k, .) (of psi(t_{k+1})). A step boundary with
+// nothing on it merges K(a_{2s-1}) with the next step's K(a_0).
+static void length_steps(qnd_ctx* c, void* psi, int64_t lst0, int64_t n, const RedFn& red_fn, bool masked) {
+    if (n <= 0) return;
+    if (c->dim == 1 && n > 1 && (masked || red_fn)) {
+        // 1-D chains carry boundary work only at their end
+        for (int64_t k = 0; k < n; ++k)
+            length_steps(c, psi, lst0 + k, 1, red_fn ? RedFn([&](int64_t, int ax) { return red_fn(k, ax); }) : RedFn(),
+                         masked);
+        return;
+    }
+    const int s = c->s;
     auto kc = [&](int i) {
         if (i == 0) return c->as[0];
-        if (i == c->s) return c->as[2 * c->s - 1];
+        if (i == s) return c->as[2 * s - 1];
         return c->as[2 * i - 1] + c->as[2 * i];
     };
-    auto spec_of = [&](int i, int ax) { return spec_table(c, SP_LENGTH, ax, kc(i)); };
-    auto mid_of = [&](int i) {
-        Factor f;
-        f.kind = RT_LENGTH;
-        f.a = c->as[2 * i] + c->as[2 * i + 1];
-        f.laser_ia = i;
-        return f;
+    std::vector<ChainK> K;
+    std::vector<ChainMid> M;
+    std::vector<std::vector<RedDesc>> reds;
+    reds.reserve(size_t(n) + 1);
+    auto reductions = [&](int64_t k) -> const RedDesc* {
+        if (!red_fn) return nullptr;
+        reds.push_back(red_fn(k, sandwich_last_axis(c, int64_t(K.size()) - 1)));
+        if (reds.back().size() > 1) QND_FAIL(QND_EINVAL, "internal: more than one reduction descriptor in a chain");
+        return reds.back().empty() ? nullptr : &reds.back()[0];
     };
-    sandwich_chain(c, psi, c->s + 1, spec_of, mid_of, Factor{}, nullptr, Factor{}, masked, fin, lst);
+    for (int64_t k = 0; k < n; ++k) {
+        const int64_t lst = lst0 + k;
+        for (int i = 0; i <= s; ++i) {
+            ChainK kk;
+            kk.kind = SP_LENGTH;
+            kk.coef = kc(i);
+            if (i == 0 && k > 0) {
+                ChainMid b;
+                b.lst = lst - 1;
+                b.mask = masked;
+                b.red = reductions(k - 1);
+                if (b.empty()) {
+                    K.back().coef += kk.coef;
+                    continue;
+                }
+                M.push_back(b);
+            } else if (i > 0) {
+                ChainMid m;
+                m.f.kind = RT_LENGTH;
+                m.f.a = c->as[2 * (i - 1)] + c->as[2 * (i - 1) + 1];
+                m.f.laser_ia = i - 1;
+                m.lst = lst;
+                M.push_back(m);
+            }
+            K.push_back(kk);
+        }
+    }
+    ChainMid post;
+    post.lst = lst0 + n - 1;
+    post.mask = masked;
+    post.red = reductions(n - 1);
+    run_chain(c, psi, K, M, Factor{}, lst0, nullptr, post);
 }
 
-// One velocity-gauge step in r-space (integrators.c:201-232).
-static void velocity_step(qnd_ctx* c, void* psi, int64_t lst, const RedDesc* fin, bool masked) {
-    auto spec_of = [&](int i, int ax) { return field_slice(c, lst, i, ax); };
-    auto mid_of = [&](int i) {
-        Factor f;
-        f.kind = RT_VEL;
-        f.a = c->as[2 * i + 1];
-        f.b = c->as[2 * i + 2];
-        return f;
-    };
-    Factor pre, post;
-    pre.kind = post.kind = RT_VEL;
+// Velocity-gauge steps lst0 .. lst0+n-1 in r-space (integrators.c:201-232); between steps the
+// factors V(a_{2s-1}) V(a_0) merge into one. The step mask and the reductions `fin` apply after the
+// last step only.
+static void velocity_steps(qnd_ctx* c, void* psi, int64_t lst0, int64_t n, const RedDesc* fin, bool masked) {
+    if (n <= 0) return;
+    const int s = c->s;
+    std::vector<ChainK> K;
+    std::vector<ChainMid> M;
+    for (int64_t k = 0; k < n; ++k)
+        for (int i = 0; i < s; ++i) {
+            if (i > 0 || k > 0) {
+                ChainMid m;
+                m.f.kind = RT_VEL;
+                m.f.a = i > 0 ? c->as[2 * i - 1] : c->as[2 * s - 1];
+                m.f.b = c->as[2 * i];
+                M.push_back(m);
+            }
+            ChainK kk;
+            kk.kind = KV_FIELD;
+            kk.lst = lst0 + k;
+            kk.ia = i;
+            K.push_back(kk);
+        }
+    Factor pre;
+    ChainMid post;
+    pre.kind = post.f.kind = RT_VEL;
     pre.a = c->as[0];
-    post.a = c->as[2 * c->s - 1];
-    sandwich_chain(c, psi, c->s, spec_of, mid_of, pre, nullptr, post, masked, fin, lst);
+    post.f.a = c->as[2 * s - 1];
+    post.lst = lst0 + n - 1;
+    post.mask = masked;
+    post.red = fin;
+    run_chain(c, psi, K, M, pre, lst0, nullptr, post);
 }
 
 static void unitary_fft(qnd_ctx* c, void* psi, bool forward) {
@@ -955,6 +1079,8 @@ static void run_realtime(qnd_ctx* c, void* psi, const double* field_host, const 
     }
     std::vector<double> zero_alpha(MAX_DIM, 0.0);
     double* rows = c->obs_dev.as<double>();
+    // length gauge whose observables are r-space reductions of one descriptor: chunk-wide chains
+    const bool chain = !velocity && (nv == 0 || (fused && rspace_red(c, items, rows, 0).size() <= 1));
     for (int64_t c0 = 0; c0 < nsteps; c0 += ch_max) {
         const int64_t ch = std::min(ch_max, nsteps - c0);
         if (nv > 0 && c0 == 0) {
@@ -962,22 +1088,35 @@ static void run_realtime(qnd_ctx* c, void* psi, const double* field_host, const 
             eval_obs(c, psi, items, al, rows);
         }
         upload_field_chunk(c, field_host + size_t(c0) * c->s * c->dim, ch, velocity);
-        for (int64_t k = 0; k < ch; ++k) {
-            const int64_t gst = c0 + k;
-            double* row = rows + size_t(k + 1) * nv;
-            std::vector<RedDesc> fin;
-            const int NK = velocity ? c->s : c->s + 1;
-            if (nv > 0 && (fused || fused_v)) fin = rspace_red(c, items, row, chain_final_axis(c, NK));
-            const RedDesc* f0 = fin.empty() ? nullptr : &fin[0];
-            if (velocity) velocity_step(c, psi, k, f0, masked);
-            else length_step(c, psi, k, f0, masked);
-            if (fin.size() > 1) {  // outputs beyond the first descriptor: a read of the final state
-                auto nat = rspace_red(c, items, row, c->dim - 1);
-                for (size_t q = 1; q < nat.size(); ++q) grid_reduce(c, psi, nat[q]);
-            }
-            if (nv > 0 && !(fused || fused_v) && gst + 1 < nsteps) {
-                const double* al = velocity ? alpha_host + size_t(gst + 1) * c->dim : zero_alpha.data();
-                eval_obs(c, psi, items, al, row);
+        if (chain) {
+            // the whole chunk is one sandwich chain; the observables of each step come out of the
+            // pass that straddles the step boundary
+            RedFn rf;
+            if (nv > 0) rf = [&](int64_t k, int ax) { return rspace_red(c, items, rows + size_t(k + 1) * nv, ax); };
+            length_steps(c, psi, 0, ch, rf, masked);
+        } else {
+            for (int64_t k = 0; k < ch; ++k) {
+                const int64_t gst = c0 + k;
+                double* row = rows + size_t(k + 1) * nv;
+                std::vector<RedDesc> fin;
+                const int NK = velocity ? c->s : c->s + 1;
+                if (nv > 0 && (fused || fused_v)) fin = rspace_red(c, items, row, chain_final_axis(c, NK));
+                const RedDesc* f0 = fin.empty() ? nullptr : &fin[0];
+                if (velocity) {
+                    velocity_steps(c, psi, k, 1, f0, masked);
+                } else {
+                    RedFn rf;
+                    if (f0) rf = [&](int64_t, int) { return std::vector<RedDesc>{*f0}; };
+                    length_steps(c, psi, k, 1, rf, masked);
+                }
+                if (fin.size() > 1) {  // outputs beyond the first descriptor: a read of the final state
+                    auto nat = rspace_red(c, items, row, c->dim - 1);
+                    for (size_t q = 1; q < nat.size(); ++q) grid_reduce(c, psi, nat[q]);
+                }
+                if (nv > 0 && !(fused || fused_v) && gst + 1 < nsteps) {
+                    const double* al = velocity ? alpha_host + size_t(gst + 1) * c->dim : zero_alpha.data();
+                    eval_obs(c, psi, items, al, row);
+                }
             }
         }
         if (nv > 0) {
@@ -1468,7 +1607,7 @@ int qnd_step_length(qnd_ctx* ctx, void* psi_p_dev, const double* E_host, int64_t
     for (int64_t c0 = 0; c0 < nsteps; c0 += CHUNK) {
         const int64_t ch = std::min(CHUNK, nsteps - c0);
         upload_field_chunk(ctx, E_host + size_t(c0) * ctx->s * ctx->dim, ch, false);
-        for (int64_t k = 0; k < ch; ++k) length_step(ctx, psi_p_dev, k, nullptr, false);
+        length_steps(ctx, psi_p_dev, 0, ch, RedFn(), false);
     }
     unitary_fft(ctx, psi_p_dev, true);
     QND_CK(cudaGetLastError());
@@ -1485,7 +1624,7 @@ int qnd_step_velocity(qnd_ctx* ctx, void* psi_dev, const double* A_host, int64_t
     for (int64_t c0 = 0; c0 < nsteps; c0 += CHUNK) {
         const int64_t ch = std::min(CHUNK, nsteps - c0);
         upload_field_chunk(ctx, A_host + size_t(c0) * ctx->s * ctx->dim, ch, true);
-        for (int64_t k = 0; k < ch; ++k) velocity_step(ctx, psi_dev, k, nullptr, false);
+        velocity_steps(ctx, psi_dev, 0, ch, nullptr, false);
     }
     QND_CK(cudaGetLastError());
     QND_API_END
@@ -1578,14 +1717,25 @@ int qnd_run_length_dev(qnd_ctx* ctx, void* psi_r_dev, const double* E_dev, int64
     const bool fused = all_rspace(items);
     const bool masked = has_mask(ctx);
     const double zero[MAX_DIM] = {0, 0, 0};
+    // observables that are r-space reductions of one descriptor: chunk-wide chains
+    const bool chain = nv == 0 || (fused && rspace_red(ctx, items, obs_dev, 0).size() <= 1);
     for (int64_t c0 = 0; c0 < nsteps; c0 += CHUNK) {
         const int64_t ch = std::min(CHUNK, nsteps - c0);
         build_field_tables(ctx, E_dev + size_t(c0) * ctx->s * ctx->dim, ch, false);
+        if (chain) {
+            RedFn rf;
+            if (nv > 0)
+                rf = [&](int64_t k, int ax) { return rspace_red(ctx, items, obs_dev + size_t(c0 + k) * nv, ax); };
+            length_steps(ctx, psi_r_dev, 0, ch, rf, masked);
+            continue;
+        }
         for (int64_t k = 0; k < ch; ++k) {
             double* row = nv > 0 ? obs_dev + size_t(c0 + k) * nv : nullptr;
             std::vector<RedDesc> fin;
             if (nv > 0 && fused) fin = rspace_red(ctx, items, row, chain_final_axis(ctx, ctx->s + 1));
-            length_step(ctx, psi_r_dev, k, fin.empty() ? nullptr : &fin[0], masked);
+            RedFn rf;
+            if (!fin.empty()) rf = [&](int64_t, int) { return std::vector<RedDesc>{fin[0]}; };
+            length_steps(ctx, psi_r_dev, k, 1, rf, masked);
             if (fin.size() > 1) {
                 auto nat = rspace_red(ctx, items, row, ctx->dim - 1);
                 for (size_t q = 1; q < nat.size(); ++q) grid_reduce(ctx, psi_r_dev, nat[q]);

@@ -72,6 +72,8 @@ template <typename R> struct PassArgs {
     const R* mid_real;           // PM_DOUBLE: r-space factors between the two sandwiches
     const V* mid_cplx;
     const V* mid_ax_cplx[MAX_DIM];
+    const R* mid_ax_real[MAX_DIM];  // PM_DOUBLE: per-axis real factors between the sandwiches (step mask)
+    int red_at_mid;                 // PM_DOUBLE: reduce the state between the sandwiches, not at the end
     const R* epi_real;
     const V* epi_cplx;
     const V* ax_cplx[MAX_DIM];   // per-axis factors (laser phases, step mask) applied ...
@@ -172,55 +174,58 @@ __device__ __forceinline__ void accumulate_red(const RedDesc& rd, double* acc, V
     }
 }
 
-// Reductions over the E values a thread holds of one line (m = tid + u*T): accumulator-outer so that
-// each accumulator's weight loads are issued together; weights along the pass axis are read per
-// element, weights along other axes once per line, full-grid weights from the line-major table.
+// Reductions over the E values a thread holds of one line (m = tid + u*T), in chunks of C values
+// (accumulator-inner within a chunk) so that few FP64 temporaries are live at once; weights along
+// the pass axis are read per element, weights along other axes once per chunk, full-grid weights
+// from the line-major table.
 template <typename R, int E, int T>
 __device__ __forceinline__ void accumulate_line(const RedDesc& rd, double* acc, const cplx_t<R>* v,
                                                 const cplx_t<R>* partner, long long base, int log2S, long long lbase,
                                                 int tid, int axis, const int* shift, const long long* nmask) {
-    double a2[E];
+    constexpr int C = E < 4 ? E : 4;
 #pragma unroll
-    for (int u = 0; u < E; ++u) a2[u] = double(v[u].x) * double(v[u].x) + double(v[u].y) * double(v[u].y);
+    for (int u0 = 0; u0 < E; u0 += C) {
+        double a2[C];
 #pragma unroll
-    for (int k = 0; k < MAX_RED; ++k) {
-        if (k >= rd.n) break;
-        double sum = 0.0;
-        const int wk = rd.wkind[k];
-        const double* __restrict__ wt = rd.wtab[k];
-        if (rd.kind[k] == RK_ABS2) {
-            if (wk == WK_ONE) {
+        for (int c = 0; c < C; ++c)
+            a2[c] = double(v[u0 + c].x) * double(v[u0 + c].x) + double(v[u0 + c].y) * double(v[u0 + c].y);
 #pragma unroll
-                for (int u = 0; u < E; ++u) sum += a2[u];
-            } else if (wk == WK_AXIS && rd.waxis[k] == axis) {
+        for (int k = 0; k < MAX_RED; ++k) {
+            if (k >= rd.n) break;
+            double sum = 0.0;
+            const int wk = rd.wkind[k];
+            const double* __restrict__ wt = rd.wtab[k];
+            if (rd.kind[k] == RK_ABS2) {
+                if (wk == WK_ONE) {
 #pragma unroll
-                for (int u = 0; u < E; ++u) sum += a2[u] * __ldg(wt + tid + u * T);
-            } else if (wk == WK_AXIS) {
-                const int ax = rd.waxis[k];
-                const double wl = __ldg(wt + ((base >> shift[ax]) & nmask[ax]));
+                    for (int c = 0; c < C; ++c) sum += a2[c];
+                } else if (wk == WK_AXIS && rd.waxis[k] == axis) {
 #pragma unroll
-                for (int u = 0; u < E; ++u) sum += a2[u];
-                sum *= wl;
+                    for (int c = 0; c < C; ++c) sum += a2[c] * __ldg(wt + tid + (u0 + c) * T);
+                } else if (wk == WK_AXIS) {
+                    const int ax = rd.waxis[k];
+                    const double wl = __ldg(wt + ((base >> shift[ax]) & nmask[ax]));
+#pragma unroll
+                    for (int c = 0; c < C; ++c) sum += a2[c];
+                    sum *= wl;
+                } else {
+#pragma unroll
+                    for (int c = 0; c < C; ++c) sum += a2[c] * __ldg(wt + lbase + tid + (u0 + c) * T);
+                }
             } else {
-                double wv[E];
 #pragma unroll
-                for (int u = 0; u < E; ++u) wv[u] = __ldg(wt + lbase + tid + u * T);
-#pragma unroll
-                for (int u = 0; u < E; ++u) sum += a2[u] * wv[u];
+                for (int c = 0; c < C; ++c) {
+                    const int m = tid + (u0 + c) * T;
+                    const long long flat = base + ((long long)m << log2S);
+                    const cplx_t<R> p = partner[flat];
+                    double val = double(p.x) * double(v[u0 + c].x) + double(p.y) * double(v[u0 + c].y);
+                    if (wk == WK_AXIS) val *= __ldg(wt + ((flat >> shift[rd.waxis[k]]) & nmask[rd.waxis[k]]));
+                    else if (wk == WK_GRID) val *= __ldg(wt + lbase + m);
+                    sum += val;
+                }
             }
-        } else {
-#pragma unroll
-            for (int u = 0; u < E; ++u) {
-                const int m = tid + u * T;
-                const long long flat = base + ((long long)m << log2S);
-                const cplx_t<R> p = partner[flat];
-                double val = double(p.x) * double(v[u].x) + double(p.y) * double(v[u].y);
-                if (wk == WK_AXIS) val *= __ldg(wt + ((flat >> shift[rd.waxis[k]]) & nmask[rd.waxis[k]]));
-                else if (wk == WK_GRID) val *= __ldg(wt + lbase + m);
-                sum += val;
-            }
+            acc[k] += sum;
         }
-        acc[k] += sum;
     }
 }
 
@@ -416,9 +421,15 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
         fft_line_stages<L, E, +1, 0, TWS>(v, tid, line, tw, lsync);
         if constexpr (MODE == PM_DOUBLE) {
             // r-space factor between the two sandwiches, then the second sandwich on the same axis
-            if (active)
-                apply_factors<R, E, T>(v, tid, base, lbase, a.mid_real, a.mid_cplx, a.mid_ax_cplx, nullptr, a.axis,
-                                       a.dim, a.shift, a.nmask, nullptr);
+            if (active) {
+                apply_factors<R, E, T>(v, tid, base, lbase, a.mid_real, a.mid_cplx, a.mid_ax_cplx, a.mid_ax_real,
+                                       a.axis, a.dim, a.shift, a.nmask, nullptr);
+                // a step boundary inside the pass: observables of the state between the two steps
+                if (a.red_at_mid && a.red.n)
+                    accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);
+            }
+            // finish those reductions here, so that no accumulator stays live through the second sandwich
+            if (a.red_at_mid && a.red.n) finish_red<NT>(a.red, acc);
             fft_line_stages<L, E, -1, 0, TWS>(v, tid, line, tw, lsync);
             if (a.spec2) {
                 const V* __restrict__ sp2 = a.spec2;
@@ -436,7 +447,7 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
                 else
                     apply_factors<R, E, T>(v, tid, base, lbase, nullptr, nullptr, nullptr, a.ax_real, a.axis, a.dim,
                                            a.shift, a.nmask, nullptr);
-                if (a.red.n)
+                if (a.red.n && !a.red_at_mid)
                     accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);
             } else {  // PM_APPLY
 #pragma unroll
@@ -481,7 +492,7 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
             for (int u = 0; u < E; ++u) out[base + tid + u * T] = v[u];
         }
     }
-    if (MODE == PM_SPECRED || a.red.n) finish_red<NT>(a.red, acc);
+    if (MODE == PM_SPECRED || (a.red.n && !a.red_at_mid)) finish_red<NT>(a.red, acc);
 }
 
 // Element-wise reductions over a whole state in r-space (no transform): norm, dipole,

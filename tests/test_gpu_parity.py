@@ -236,3 +236,122 @@ def test_mixed_precision_error_bound(Grid, shape, dr):
     assert rel(st.download(), a) < 2e-5
     scale = np.maximum(np.abs(ob_o), 1e-3)
     assert np.max(np.abs(ob_m - ob_o) / scale) < 5e-6
+
+
+def cos8_mask(axis, frac=0.1):
+    """cos^(1/8) absorbing mask over the outer `frac` of an axis (the benchmark's mask)."""
+    half = np.max(np.abs(axis))
+    edge = (1.0 - frac) * half
+    m = np.ones_like(axis)
+    zone = np.abs(axis) > edge
+    m[zone] = np.cos(0.5 * np.pi * (np.abs(axis[zone]) - edge) / (half - edge)).clip(0.0) ** 0.125
+    return m
+
+
+def _masked_pair(Grid, shape, dr, integ="BM4"):
+    dim = len(shape)
+    grid = Grid(dim, shape, dr, integ, 0.05)
+    V, grads = soft_coulomb(grid, 0.64)
+    o = O.OracleCtx(dim, shape, dr, integ, 0.05)
+    for ctx in (grid, o):
+        if ctx is grid:
+            ctx.set_potential(V)
+        else:
+            ctx.set_vpot(V)
+        ctx.set_cap(0.05, 2.0)
+        for j in range(dim):
+            ctx.set_gradv(j, grads[j])
+            ctx.set_mask_axis(j, cos8_mask(grid.axis_r(j)))
+    return grid, o
+
+
+@pytest.mark.parametrize("shape,dr", [((256, 256), (0.2, 0.2)), ((16, 32, 64), (0.5, 0.4, 0.3)), ((2048,), (0.1,)),
+                                      ((64, 2048), (0.4, 0.1))])
+def test_masked_run_with_observables_vs_oracle(Grid, shape, dr):
+    """Several steps in one sandwich chain: the step mask and each step's observables are applied
+    inside the pass that straddles the step boundary (2-D, 3-D); per-step chains in 1-D."""
+    grid, o = _masked_pair(Grid, shape, dr)
+    dim = len(shape)
+    psi0 = O.smooth_state(shape, dr, 6)
+    nsteps = 5
+    E = np.random.default_rng(7).standard_normal((nsteps, grid.s, dim)) * 0.05
+    names = ["norm", "dipole_r", "accel"]
+    a = psi0.copy()
+    ob_o = o.run_length(a, E, names)
+    st = grid.state(psi0)
+    ob_g = grid.run_length(st, E, names)
+    assert rel(st.download(), a) < TOL
+    np.testing.assert_allclose(ob_g, ob_o, rtol=1e-11, atol=1e-13)
+
+
+def test_device_loop_matches_host_loop_masked(Grid):
+    """qnd_run_length_dev (rows after each step, device buffers) against qnd_run_length (rows before
+    each step) on the same masked run: row i of the first is row i+1 of the second."""
+    import torch
+
+    shape, dr = (512, 512), (0.2, 0.2)
+    grid, _ = _masked_pair(Grid, shape, dr)
+    psi0 = O.smooth_state(shape, dr, 8)
+    nsteps = 6
+    E = np.random.default_rng(9).standard_normal((nsteps + 1, grid.s, 2)) * 0.05
+    names = ["norm", "dipole_r", "accel"]
+    st = grid.state(psi0)
+    ob_host = grid.run_length(st, E, names)
+    psi_host = st.download()
+    st2 = grid.state(psi0)
+    E_dev = torch.tensor(E, device="cuda")
+    obs_dev = torch.zeros((nsteps + 1, ob_host.shape[1]), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    grid.run_length_dev(st2, E_dev, nsteps + 1, names, obs_dev)
+    grid.synchronize()
+    np.testing.assert_allclose(obs_dev.cpu().numpy()[:nsteps], ob_host[1:], rtol=1e-12, atol=1e-15)
+    assert rel(st2.download(), psi_host) < 1e-13
+
+
+def test_many_observable_values_fall_back_per_step(Grid):
+    """More reduction outputs than one fused descriptor holds (3-D: 10 values): per-step chains
+    with an extra grid reduction, same results."""
+    shape, dr = (16, 32, 32), (0.5, 0.4, 0.4)
+    grid, o = _masked_pair(Grid, shape, dr)
+    psi0 = O.smooth_state(shape, dr, 10)
+    E = np.random.default_rng(11).standard_normal((3, grid.s, 3)) * 0.05
+    names = ["norm", "dipole_r", "accel", "dipole_r"]
+    a = psi0.copy()
+    ob_o = o.run_length(a, E, names)
+    st = grid.state(psi0)
+    ob_g = grid.run_length(st, E, names)
+    assert rel(st.download(), a) < TOL
+    np.testing.assert_allclose(ob_g, ob_o, rtol=1e-11, atol=1e-13)
+
+
+@pytest.mark.parametrize("shape,dr", [((128, 256), (0.3, 0.2)), ((1024,), (0.2,)), ((16, 16, 32), (0.5, 0.5, 0.4))])
+def test_multistep_length_velocity_imag_vs_oracle(Grid, shape, dr):
+    """Multi-step calls without observables or mask: consecutive steps merge K(a_2s-1) K(a_0) into one
+    sandwich (length gauge) or V(a_2s-1) V(a_0) into one factor (velocity, imaginary time)."""
+    dim = len(shape)
+    grid = Grid(dim, shape, dr, "BM4", 0.05)
+    grid.set_potential(POT[{1: "1d", 2: "2d", 3: "3d"}[dim]])
+    grid.set_cap(0.1, 1.0)
+    o = O.OracleCtx(dim, shape, dr, "BM4", 0.05)
+    o.set_potential(POT[{1: "1d", 2: "2d", 3: "3d"}[dim]])
+    o.set_cap(0.1, 1.0)
+    psi0 = O.smooth_state(shape, dr, 12)
+    n = 4
+    F = np.random.default_rng(13).standard_normal((n, grid.s, dim)) * 0.05
+    a = psi0.copy()
+    o.to_p(a)
+    o.step_length(a, F, n)
+    st = grid.state(psi0)
+    grid.to_p(st)
+    grid.integration_step_length(st, F)
+    assert rel(st.download(), a) < TOL
+    a = psi0.copy()
+    o.step_velocity(a, F * 5, n)
+    st.upload(psi0)
+    grid.integration_step_velocity(st, F * 5)
+    assert rel(st.download(), a) < TOL
+    a = psi0.copy()
+    o.step_imag(a, n)
+    st.upload(psi0)
+    grid.integration_step_imag(st, n)
+    assert rel(st.download(), a) < TOL
