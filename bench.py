@@ -292,10 +292,16 @@ def ground_state(torch, V, stream, nsteps):
 BLOCK = 100  # consecutive steps per timed call (one device-resident chain); the L2 is flushed between calls
 
 
-def timed_steps(torch, grid, psi_t, E_dev, obs_dev, names, i0, steps, warmup, flush, block=BLOCK):
+def timed_steps(torch, grid, psi_t, E_dev, obs_dev, names, i0, steps, warmup, flush, block=BLOCK, graph=True):
     """Warm-up, then `steps` steps as calls of `block` consecutive steps (the last one shorter), each
     call bracketed by CUDA events and preceded by an untimed 256 MB write that flushes the L2. Within a
-    call the state stays on chip between steps, as in a long propagation."""
+    call the state stays on chip between steps, as in a long propagation.
+
+    Each call of `block` steps is one qnd_run_length_dev chain captured once in a CUDA graph (after
+    a warm-up call has built the tables) and replayed; the timed region of a call holds the copy of
+    its field samples into the graph's input buffer, the replay and the copy of its observable rows
+    out, so that the measurement does not depend on how fast the host enqueues launches. With
+    graph=False every call is enqueued directly (the per-launch profiling run)."""
     def calls(n, first):
         k = 0
         while k < n:
@@ -306,14 +312,63 @@ def timed_steps(torch, grid, psi_t, E_dev, obs_dev, names, i0, steps, warmup, fl
         flush.zero_()
         grid.run_length_dev(psi_t, E_dev[i0 + k:i0 + k + b], b, names, obs_dev[k:k + b])
     torch.cuda.synchronize()
+    if not graph:
+        todo = list(calls(steps, warmup))
+        starts = [torch.cuda.Event(enable_timing=True) for _ in todo]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in todo]
+        for (k, b), st, en in zip(todo, starts, ends):
+            flush.zero_()
+            st.record()
+            grid.run_length_dev(psi_t, E_dev[i0 + k:i0 + k + b], b, names, obs_dev[k:k + b])
+            en.record()
+        torch.cuda.synchronize()
+        return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    graphs = {}
+
+    def graph_for(b):
+        if b not in graphs:
+            e_buf = torch.empty_like(E_dev[:b])
+            o_buf = torch.empty_like(obs_dev[:b])
+            e_buf.copy_(E_dev[i0:i0 + b])
+            grid.run_length_dev(psi_t.clone(), e_buf, b, names, o_buf)   # tables for this shape
+            torch.cuda.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=torch.cuda.current_stream()):
+                grid.run_length_dev(psi_t, e_buf, b, names, o_buf)
+            graphs[b] = (g, e_buf, o_buf)
+        return graphs[b]
+
     todo = list(calls(steps, warmup))
+    for _, b in todo:
+        graph_for(b)
+    torch.cuda.synchronize()
     starts = [torch.cuda.Event(enable_timing=True) for _ in todo]
     ends = [torch.cuda.Event(enable_timing=True) for _ in todo]
     for (k, b), st, en in zip(todo, starts, ends):
+        g, e_buf, o_buf = graphs[b]
         flush.zero_()
         st.record()
-        grid.run_length_dev(psi_t, E_dev[i0 + k:i0 + k + b], b, names, obs_dev[k:k + b])
+        e_buf.copy_(E_dev[i0 + k:i0 + k + b])
+        g.replay()
+        obs_dev[k:k + b].copy_(o_buf)
         en.record()
+    torch.cuda.synchronize()
+    total = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    graphs.clear()
+    return total
+
+
+def timed_steps_single(torch, grid, psi_t, E_dev, obs_dev, names, i0, steps, flush):
+    """`steps` single-step qnd_run_length_dev calls, each bracketed by CUDA events, the L2 flushed
+    before every step (no on-chip state across steps; host enqueue included)."""
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    torch.cuda.synchronize()
+    for k in range(steps):
+        flush.zero_()
+        starts[k].record()
+        grid.run_length_dev(psi_t, E_dev[i0 + k:i0 + k + 1], 1, names, obs_dev[k:k + 1])
+        ends[k].record()
     torch.cuda.synchronize()
     return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
 
@@ -369,9 +424,7 @@ def main():
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         total_ms = timed_steps(torch, grid, psi_t, E_dev, obs_dev, OBS, i0, args.steps, args.warmup, flush)
-    launches, _, _ = grid.get_profile(reset=True)
-    per_step_launches = launches / (args.steps + args.warmup)
-    gpu_launches = int(round(per_step_launches * args.steps))
+    grid.get_profile(reset=True)
     if dist:
         tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -384,13 +437,15 @@ def main():
     grid.set_profiling(True)
     prof_steps = min(args.steps, 100)
     psi_t2 = torch.tensor(psi0.view(np.float64), device=dev).contiguous()
-    timed_steps(torch, grid, psi_t2, E_dev, obs_dev, OBS, i0, prof_steps, 0, flush)
-    _, passes, pass_ms = grid.get_profile(reset=True)
+    timed_steps(torch, grid, psi_t2, E_dev, obs_dev, OBS, i0, prof_steps, 0, flush, graph=False)
+    prof_kernels, passes, pass_ms = grid.get_profile(reset=True)
     grid.set_profiling(False)
+    # our kernels per step, counted on the plain-call run (graph replays launch the same kernels)
+    gpu_launches = int(round(prof_kernels / prof_steps * args.steps))
     # the same steps one call per step with the L2 flushed before each (no on-chip state across steps)
     fs_steps = min(args.steps, 100)
     psi_t3 = torch.tensor(psi0.view(np.float64), device=dev).contiguous()
-    ms_fs = timed_steps(torch, grid, psi_t3, E_dev, obs_dev, OBS, i0, fs_steps, 0, flush, block=1) / fs_steps
+    ms_fs = timed_steps_single(torch, grid, psi_t3, E_dev, obs_dev, OBS, i0, fs_steps, flush) / fs_steps
     flush_every_step = {"value": 1000.0 / ms_fs, "unit": "steps/s", "ms_per_step": ms_fs, "steps": fs_steps,
                         "what": "rank-local: one qnd_run_length_dev call per step, 256 MB L2 flush before each step"}
     n = NR * NR
@@ -435,10 +490,14 @@ def main():
         dist.barrier()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record()
+    h0 = time.perf_counter()
     _lib.check(L.qnd_state_upload(grid.h, C.c_void_p(psi_dev_e2e.data_ptr()), dptr(psi_host)))
+    h1 = time.perf_counter()
     _lib.check(L.qnd_run_length(grid.h, C.c_void_p(psi_dev_e2e.data_ptr()), dptr(E_host), e2e_steps, len(OBS),
                                 names_c, dptr(obs_host)))
+    h2 = time.perf_counter()
     _lib.check(L.qnd_state_download(grid.h, dptr(psi_host), C.c_void_p(psi_dev_e2e.data_ptr())))
+    h3 = time.perf_counter()
     b.record()
     torch.cuda.synchronize()
     e2e_ms = a.elapsed_time(b)
@@ -449,7 +508,8 @@ def main():
     e2e = {"value": world * e2e_steps / (e2e_ms / 1000.0), "unit": "steps/s",
            "h2d_bytes_per_step": (n * 16 + e2e_steps * grid.s * 2 * 8) / e2e_steps,
            "d2h_bytes_per_step": (n * 16 + e2e_steps * nv * 8) / e2e_steps,
-           "what": "qnd_state_upload + qnd_run_length (host E, host observable rows) + qnd_state_download"}
+           "what": "qnd_state_upload + qnd_run_length (host E, host observable rows) + qnd_state_download",
+           "host_ms": {"upload": 1e3 * (h1 - h0), "run_length": 1e3 * (h2 - h1), "download": 1e3 * (h3 - h2)}}
 
     extras = {}
     if not args.no_extras:

@@ -104,9 +104,17 @@ __global__ void __launch_bounds__(256) field_tables_kernel(const __grid_constant
             theta = h * (x * f);
             mag = 1.0;
         }
-        double sn, cs;
-        sincos(theta, &sn, &cs);
-        out[i] = cplx_t<R>{R(mag * cs), R(-mag * sn)};
+        if constexpr (sizeof(R) == 4) {
+            // FP32 factors are stored as d = e^{-i theta} - 1 (the velocity tables' 1/N is applied
+            // as the spectral scaling): cos - 1 = -2 sin^2(theta/2)
+            double sh, ch;
+            sincos(0.5 * theta, &sh, &ch);
+            out[i] = cplx_t<R>{R(-2.0 * sh * sh), R(-2.0 * sh * ch)};
+        } else {
+            double sn, cs;
+            sincos(theta, &sn, &cs);
+            out[i] = cplx_t<R>{R(mag * cs), R(-mag * sn)};
+        }
     }
 }
 
@@ -125,7 +133,9 @@ __global__ void axis_table_kernel(int mode, const double* p, int N, double alpha
         if (mode == 0) {
             static_cast<double*>(out)[k] = w;
         } else {
-            static_cast<cplx_t<R>*>(out)[k] = cplx_t<R>{R(w / double(N)), R(0)};
+            // a spectral factor: FP32 tables hold w N - 1 (see fmul_spec)
+            static_cast<cplx_t<R>*>(out)[k] = sizeof(R) == 8 ? cplx_t<R>{R(w / double(N)), R(0)}
+                                                             : cplx_t<R>{R(w - 1.0), R(0)};
         }
     }
 }

@@ -157,6 +157,15 @@ struct qnd_ctx {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pairs;
     std::vector<cudaEvent_t> event_pool;
 
+    // A chunk-wide sandwich chain captured in a CUDA graph and replayed for the later chunks of the
+    // same shape: what it captured (key), the executable graph, the kernels one replay launches,
+    // and the key of the last chain run directly (its tables exist). config_epoch bumps with every
+    // setter that changes what a chain reads.
+    std::string chain_key, chain_warm;
+    cudaGraphExec_t chain_exec = nullptr;
+    int64_t chain_launches = 0;
+    uint64_t config_epoch = 0;
+
     size_t elem() const { return fp64 ? 16 : 8; }
     size_t rsize() const { return fp64 ? 8 : 4; }
 };
@@ -164,6 +173,51 @@ struct qnd_ctx {
 namespace qnd {
 
 // ---------------------------------------------------------------- tables --
+
+// Rounds n stored FP32 factors d (interleaved doubles; the factor is 1 + d, see fmul in
+// qnd_fft.cuh) to float pairs so that the squared magnitudes |1 + d|^2 of the rounded values add up
+// to those of the exact ones along the array: each value takes, among the 5 x 5 neighbourhood of its
+// nearest-rounded parts, the pair that brings the running sum of magnitude errors closest to zero
+// (ties: the nearer pair). Every contiguous run of entries then carries a magnitude error bounded
+// by two single-entry errors in total, so the FFT stage twiddles and the phase tables applied at
+// every step leave no systematic drift of the norm. Each part stays within two units in the last
+// place.
+static void round_pairs_f32_balanced(const double* v, size_t n, float* out) {
+    double run = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+        const double re = v[2 * i], im = v[2 * i + 1];
+        // |1 + x|^2 - |1 + d|^2 = (xr - dr)(2 + xr + dr) + (xi - di)(xi + di)
+        auto merr = [&](double xr, double xi) { return (xr - re) * (2.0 + xr + re) + (xi - im) * (xi + im); };
+        float rs[5], is[5];
+        rs[2] = float(re);
+        is[2] = float(im);
+        rs[1] = std::nextafter(rs[2], -INFINITY);
+        rs[0] = std::nextafter(rs[1], -INFINITY);
+        rs[3] = std::nextafter(rs[2], INFINITY);
+        rs[4] = std::nextafter(rs[3], INFINITY);
+        is[1] = std::nextafter(is[2], -INFINITY);
+        is[0] = std::nextafter(is[1], -INFINITY);
+        is[3] = std::nextafter(is[2], INFINITY);
+        is[4] = std::nextafter(is[3], INFINITY);
+        float br = rs[2], bi = is[2];
+        double be = std::fabs(run + merr(br, bi)), bd = 1e300;
+        for (int a = 0; a < 5; ++a)
+            for (int q = 0; q < 5; ++q) {
+                const double xr = rs[a], xi = is[q];
+                const double e = std::fabs(run + merr(xr, xi));
+                const double d = (xr - re) * (xr - re) + (xi - im) * (xi - im);
+                if (e < be || (e == be && d < bd)) {
+                    be = e;
+                    bd = d;
+                    br = rs[a];
+                    bi = is[q];
+                }
+            }
+        run += merr(br, bi);
+        out[2 * i] = br;
+        out[2 * i + 1] = bi;
+    }
+}
 
 // Twiddles of HostPlan(L) in the [j mod Ns][r-1] layout, exp(-2 pi i jm r / (Ns R)), in long double.
 static void build_twiddles(qnd_ctx* c, int ax) {
@@ -177,7 +231,12 @@ static void build_twiddles(qnd_ctx* c, int ax) {
         for (int jm = 0; jm < Ns; ++jm)
             for (int r = 1; r < R; ++r) {
                 long double ang = two_pi * (long double)(jm * r) / (long double)(Ns * R);
-                tw[2 * o] = (double)cosl(ang);
+                if (c->fp64) {
+                    tw[2 * o] = (double)cosl(ang);
+                } else {  // stored as w - 1 (cos - 1 = -2 sin^2(ang/2))
+                    const long double sh = sinl(ang / 2);
+                    tw[2 * o] = (double)(-2 * sh * sh);
+                }
                 tw[2 * o + 1] = (double)(-sinl(ang));
                 ++o;
             }
@@ -188,12 +247,13 @@ static void build_twiddles(qnd_ctx* c, int ax) {
         QND_CK(cudaMemcpyAsync(c->tw[ax].p, tw.data(), cnt * 16, cudaMemcpyHostToDevice, c->stream));
     } else {
         std::vector<float> f(2 * cnt);
-        for (size_t i = 0; i < 2 * cnt; ++i) f[i] = float(tw[i]);
+        round_pairs_f32_balanced(tw.data(), cnt, f.data());
         QND_CK(cudaMemcpyAsync(c->tw[ax].p, f.data(), cnt * 8, cudaMemcpyHostToDevice, c->stream));
     }
 }
 
-// Upload n complex values given as interleaved doubles, converting to the context precision.
+// Upload n stored complex factors given as interleaved doubles: the factors w themselves for FP64
+// contexts, d = w - 1 (spectral tables: w N_axis - 1) for FP32 contexts.
 static void upload_cplx(qnd_ctx* c, DevBuf& dst, const std::vector<double>& v) {
     const size_t n = v.size() / 2;
     dst.ensure(n * c->elem());
@@ -201,11 +261,10 @@ static void upload_cplx(qnd_ctx* c, DevBuf& dst, const std::vector<double>& v) {
         QND_CK(cudaMemcpyAsync(dst.p, v.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
     } else {
         std::vector<float> f(2 * n);
-        for (size_t i = 0; i < 2 * n; ++i) {
-            f[i] = float(v[i]);
-            if (std::isinf(f[i]) && !std::isinf(v[i]))
+        for (size_t i = 0; i < 2 * n; ++i)
+            if (std::isinf(float(v[i])) && !std::isinf(v[i]))
                 QND_FAIL(QND_EUNSUPPORTED, "a phase/decay factor exceeds the FP32 range: use QND_FP64 for this case");
-        }
+        round_pairs_f32_balanced(v.data(), n, f.data());
         QND_CK(cudaMemcpyAsync(dst.p, f.data(), n * 8, cudaMemcpyHostToDevice, c->stream));
     }
 }
@@ -251,13 +310,18 @@ static const void* spec_table(qnd_ctx* c, int kind, int ax, double coef) {
         double re, im;
         if (kind == SP_LENGTH) {
             const double th = coef * kin;
-            re = std::cos(th) / N;
-            im = -std::sin(th) / N;
+            if (c->fp64) {
+                re = std::cos(th) / N;
+            } else {
+                const double sh = std::sin(th / 2);
+                re = -2 * sh * sh;
+            }
+            im = c->fp64 ? -std::sin(th) / N : -std::sin(th);
         } else if (kind == SP_IMAG) {
-            re = std::exp(-coef * kin) / N;
+            re = c->fp64 ? std::exp(-coef * kin) / N : std::expm1(-coef * kin);
             im = 0;
         } else {
-            re = kin / N;
+            re = c->fp64 ? kin / N : kin - 1.0;
             im = 0;
         }
         v[2 * k] = re;
@@ -302,6 +366,15 @@ static const void* rtab(qnd_ctx* c, int kind, double a, double b, int ax);
 // Full-grid tables in the natural layout (the contiguous axis' line-major layout).
 static const void* rtab(qnd_ctx* c, int kind, double a, double b) { return rtab(c, kind, a, b, c->dim - 1); }
 
+// d = w - 1 for w = exp(x) e^{-i th} (x = the clamped CAP exponent), computed without cancellation:
+// Re d = (e^x - 1) cos th + (cos th - 1), Im d = -e^x sin th.
+static void unit_factor_d(double x, double th, double* dr, double* di) {
+    const double em1 = x > MAX_EXP_ARG ? std::exp(MAX_EXP_ARG) - 1.0 : std::expm1(x);
+    const double sh = std::sin(th / 2);
+    *dr = em1 * std::cos(th) - 2 * sh * sh;
+    *di = -(em1 + 1.0) * std::sin(th);
+}
+
 static const void* rtab(qnd_ctx* c, int kind, double a, double b, int ax) {
     auto key = std::make_tuple(kind * 8 + ax, a, b, c->table_epoch);
     auto it = c->rtab_cache.find(key);
@@ -322,21 +395,36 @@ static const void* rtab(qnd_ctx* c, int kind, double a, double b, int ax) {
         for (size_t i = 0; i < n; ++i) {
             const double vc = c->vcap.empty() ? 0.0 : c->vcap[i];
             double re, im;
-            if (kind == RT_LENGTH) {
-                const double m = clamped_exp(-a * vc), th = a * c->vpot[i];
-                re = m * std::cos(th);
-                im = -m * std::sin(th);
-            } else {
-                const double m1 = clamped_exp(-a * vc), th1 = a * c->vpot[i];
-                re = m1 * std::cos(th1);
-                im = -m1 * std::sin(th1);
-                if (b != NO_COEF) {
-                    const double m2 = clamped_exp(-b * vc), th2 = b * c->vpot[i];
-                    const double r2 = m2 * std::cos(th2), i2 = -m2 * std::sin(th2);
-                    const double nr_ = re * r2 - im * i2, ni = re * i2 + im * r2;
-                    re = nr_;
-                    im = ni;
+            if (c->fp64) {
+                if (kind == RT_LENGTH) {
+                    const double m = clamped_exp(-a * vc), th = a * c->vpot[i];
+                    re = m * std::cos(th);
+                    im = -m * std::sin(th);
+                } else {
+                    const double m1 = clamped_exp(-a * vc), th1 = a * c->vpot[i];
+                    re = m1 * std::cos(th1);
+                    im = -m1 * std::sin(th1);
+                    if (b != NO_COEF) {
+                        const double m2 = clamped_exp(-b * vc), th2 = b * c->vpot[i];
+                        const double r2 = m2 * std::cos(th2), i2 = -m2 * std::sin(th2);
+                        const double nr_ = re * r2 - im * i2, ni = re * i2 + im * r2;
+                        re = nr_;
+                        im = ni;
+                    }
                 }
+            } else {
+                // FP32 factors are stored as d = w - 1 (one factor, or the product of two)
+                double dr, di;
+                unit_factor_d(-a * vc, a * c->vpot[i], &dr, &di);
+                if (kind == RT_VEL && b != NO_COEF) {
+                    double er, ei;
+                    unit_factor_d(-b * vc, b * c->vpot[i], &er, &ei);
+                    const double pr = dr * er - di * ei, pi = dr * ei + di * er;
+                    dr = dr + er + pr;
+                    di = di + ei + pi;
+                }
+                re = dr;
+                im = di;
             }
             v[2 * i] = re;
             v[2 * i + 1] = im;
@@ -425,6 +513,7 @@ template <typename R> static void fill_args(qnd_ctx* c, const PassSpec& ps, Pass
     a.scale = R(ps.scale);
     a.apply_acc = ps.apply_acc;
     a.apply_vtab = ps.apply_vtab;
+    a.seed = uint32_t(c->kernels_launched) * 0x9e3779b9u + 0x632be5abu;
     a.red = ps.red;
 }
 
@@ -1064,6 +1153,72 @@ static void unitary_fft(qnd_ctx* c, void* psi, bool forward) {
 
 static const int64_t CHUNK = 128;
 
+// Run a chunk-wide chain (body) through a CUDA graph. The first run of a key goes directly (it
+// builds the tables the chain reads); the second captures it; later runs replay the graph, so the
+// host enqueues one graph launch per chunk instead of ~7 kernels per step and the device does not
+// wait on a slow host. Direct runs when profiling (per-launch events), when the caller is already
+// capturing the stream, or with QND_NO_GRAPH set.
+static void run_chunk_graph(qnd_ctx* c, const std::string& key, const std::function<void()>& body) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    QND_CK(cudaStreamIsCapturing(c->stream, &cs));
+    if (c->profiling || cs != cudaStreamCaptureStatusNone || std::getenv("QND_NO_GRAPH")) {
+        body();
+        return;
+    }
+    if (c->chain_exec && c->chain_key == key) {
+        QND_CK(cudaGraphLaunch(c->chain_exec, c->stream));
+        c->kernels_launched += c->chain_launches;
+        return;
+    }
+    if (c->chain_warm != key) {
+        body();
+        c->chain_warm = key;
+        return;
+    }
+    if (c->chain_exec) {
+        cudaGraphExecDestroy(c->chain_exec);
+        c->chain_exec = nullptr;
+        c->chain_key.clear();
+    }
+    const int64_t k0 = c->kernels_launched;
+    QND_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    cudaGraph_t g = nullptr;
+    try {
+        body();
+    } catch (...) {
+        cudaStreamEndCapture(c->stream, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        c->kernels_launched = k0;
+        throw;
+    }
+    QND_CK(cudaStreamEndCapture(c->stream, &g));
+    cudaGraphExec_t ex = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        QND_FAIL(QND_ECUDA, "cudaGraphInstantiate of a step chain: %s", cudaGetErrorString(e));
+    }
+    c->chain_exec = ex;
+    c->chain_key = key;
+    c->chain_launches = c->kernels_launched - k0;
+    QND_CK(cudaGraphLaunch(ex, c->stream));
+}
+
+// What a length-gauge chunk chain captures (see run_chunk_graph).
+static std::string chain_key(qnd_ctx* c, const void* psi, int64_t ch, int nobs, const char* const* names,
+                             const double* rows, bool masked) {
+    std::string k = fmt("L|%p|%lld|%p|%d|%p|%p|%p|%llu|%llu|%d|", psi, (long long)ch, (const void*)rows, int(masked),
+                        c->field_tab.p, c->partials.p, c->counter.p, (unsigned long long)c->table_epoch,
+                        (unsigned long long)c->config_epoch, int(c->pdl));
+    for (int q = 0; q < nobs; ++q) {
+        k += names[q] ? names[q] : "";
+        k += ',';
+    }
+    return k;
+}
+
 // Real-time driver loop (QuantumND_real.c:168-229) for either gauge.
 static void run_realtime(qnd_ctx* c, void* psi, const double* field_host, const double* alpha_host, int64_t nsteps,
                          int nobs, const char* const* names, double* obs_host, bool velocity) {
@@ -1093,7 +1248,8 @@ static void run_realtime(qnd_ctx* c, void* psi, const double* field_host, const 
             // pass that straddles the step boundary
             RedFn rf;
             if (nv > 0) rf = [&](int64_t k, int ax) { return rspace_red(c, items, rows + size_t(k + 1) * nv, ax); };
-            length_steps(c, psi, 0, ch, rf, masked);
+            run_chunk_graph(c, chain_key(c, psi, ch, nobs, names, rows, masked),
+                            [&]() { length_steps(c, psi, 0, ch, rf, masked); });
         } else {
             for (int64_t k = 0; k < ch; ++k) {
                 const int64_t gst = c0 + k;
@@ -1350,6 +1506,7 @@ int qnd_ctx_destroy(qnd_ctx* ctx) {
         cudaEventDestroy(pr.second);
     }
     for (auto e : ctx->event_pool) cudaEventDestroy(e);
+    if (ctx->chain_exec) cudaGraphExecDestroy(ctx->chain_exec);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     QND_API_END
@@ -1358,6 +1515,7 @@ int qnd_ctx_destroy(qnd_ctx* ctx) {
 int qnd_ctx_set_stream(qnd_ctx* ctx, void* stream) {
     QND_API_BEGIN
     QND_NEED(ctx);
+    ctx->config_epoch++;
     set_device(ctx);
     QND_CK(cudaStreamSynchronize(ctx->stream));
     if (stream) {
@@ -1394,6 +1552,7 @@ int qnd_state_bytes(qnd_ctx* ctx, int64_t* bytes) {
 int qnd_set_potential_named(qnd_ctx* ctx, const char* name) {
     QND_API_BEGIN
     QND_NEED(ctx);
+    ctx->config_epoch++;
     QND_NEED(name);
     double probe;
     if (!named_potential(name, 0.0, &probe)) QND_FAIL(QND_EINVAL, "Unknown potential: %s", name);
@@ -1422,6 +1581,7 @@ int qnd_set_potential_named(qnd_ctx* ctx, const char* name) {
 int qnd_set_potential(qnd_ctx* ctx, const double* vpot_host) {
     QND_API_BEGIN
     QND_NEED(ctx);
+    ctx->config_epoch++;
     QND_NEED(vpot_host);
     ctx->vpot.assign(vpot_host, vpot_host + ctx->n);
     ctx->vpot_dev.reset();
@@ -1432,6 +1592,7 @@ int qnd_set_potential(qnd_ctx* ctx, const double* vpot_host) {
 int qnd_set_cap(qnd_ctx* ctx, double strength, double length) {
     QND_API_BEGIN
     QND_NEED(ctx);
+    ctx->config_epoch++;
     std::vector<double> v(size_t(ctx->n), 0.0);
     int64_t idx[MAX_DIM];
     for (int64_t i = 0; i < ctx->n; ++i) {
@@ -1456,6 +1617,7 @@ int qnd_set_cap(qnd_ctx* ctx, double strength, double length) {
 int qnd_set_vcap(qnd_ctx* ctx, const double* vcap_host) {
     QND_API_BEGIN
     QND_NEED(ctx);
+    ctx->config_epoch++;
     if (vcap_host) ctx->vcap.assign(vcap_host, vcap_host + ctx->n);
     else ctx->vcap.clear();
     invalidate_rtabs(ctx);
@@ -1465,6 +1627,7 @@ int qnd_set_vcap(qnd_ctx* ctx, const double* vcap_host) {
 int qnd_set_gradv(qnd_ctx* ctx, int axis, const double* gradv_host) {
     QND_API_BEGIN
     QND_NEED(ctx);
+    ctx->config_epoch++;
     if (axis < 0 || axis >= ctx->dim) QND_FAIL(QND_EINVAL, "axis %d out of range", axis);
     set_device(ctx);
     if (!gradv_host) {
@@ -1482,6 +1645,7 @@ int qnd_set_gradv(qnd_ctx* ctx, int axis, const double* gradv_host) {
 int qnd_set_mask_axis(qnd_ctx* ctx, int axis, const double* mask_host) {
     QND_API_BEGIN
     QND_NEED(ctx);
+    ctx->config_epoch++;
     if (axis < 0 || axis >= ctx->dim) QND_FAIL(QND_EINVAL, "axis %d out of range", axis);
     set_device(ctx);
     if (!mask_host) {
@@ -1723,10 +1887,20 @@ int qnd_run_length_dev(qnd_ctx* ctx, void* psi_r_dev, const double* E_dev, int64
         const int64_t ch = std::min(CHUNK, nsteps - c0);
         build_field_tables(ctx, E_dev + size_t(c0) * ctx->s * ctx->dim, ch, false);
         if (chain) {
+            // rows are staged in the context's buffer (fixed addresses, so that a captured chain
+            // replays for every chunk), then copied to obs_dev
+            double* stage = nullptr;
+            if (nv > 0) {
+                ctx->obs_dev.ensure(size_t(CHUNK) * nv * sizeof(double));
+                stage = ctx->obs_dev.as<double>();
+            }
             RedFn rf;
+            if (nv > 0) rf = [&](int64_t k, int ax) { return rspace_red(ctx, items, stage + size_t(k) * nv, ax); };
+            run_chunk_graph(ctx, chain_key(ctx, psi_r_dev, ch, nobs, names, stage, masked),
+                            [&]() { length_steps(ctx, psi_r_dev, 0, ch, rf, masked); });
             if (nv > 0)
-                rf = [&](int64_t k, int ax) { return rspace_red(ctx, items, obs_dev + size_t(c0 + k) * nv, ax); };
-            length_steps(ctx, psi_r_dev, 0, ch, rf, masked);
+                QND_CK(cudaMemcpyAsync(obs_dev + size_t(c0) * nv, stage, size_t(ch) * nv * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, ctx->stream));
             continue;
         }
         for (int64_t k = 0; k < ch; ++k) {

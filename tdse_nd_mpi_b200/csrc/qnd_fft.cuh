@@ -43,6 +43,74 @@ template <typename V> __device__ __forceinline__ V cmulc(V a, V b) {
 }
 template <typename V, typename S> __device__ __forceinline__ V cscale(V a, S s) { return V{a.x * s, a.y * s}; }
 
+// Stored complex factors. FP64 tables hold the factor w itself. FP32 tables hold d = w - 1 (for the
+// spectral tables, d = w N_axis - 1, the 1/N_axis applied as an exact power-of-two scaling): then
+// x w = x + x d. A near-unit factor (a small phase: the entries that a smooth state weights most)
+// rounded as d keeps its magnitude exact to a few units in the last place of d rather than of 1,
+// which removes the systematic FP32 norm drift that rounding w itself leaves (about 1e-7 per BM4
+// step). The product costs the same four fused multiply-adds as cmul.
+template <typename V> __device__ __forceinline__ V fmul(V x, V f) {
+    if constexpr (sizeof(x.x) == 8) {
+        return cmul(x, f);
+    } else {
+        return V{fmaf(x.x, f.x, fmaf(-x.y, f.y, x.x)), fmaf(x.x, f.y, fmaf(x.y, f.x, x.y))};
+    }
+}
+// The factor of a product of two stored factors, in the same representation.
+template <typename V> __device__ __forceinline__ V fcompose(V f, V g) {
+    if constexpr (sizeof(f.x) == 8) {
+        return cmul(f, g);
+    } else {
+        return cadd(cadd(f, g), cmul(f, g));
+    }
+}
+// The stored representation of the factor 1.
+template <typename V> __device__ __forceinline__ V fone() {
+    if constexpr (sizeof(V{}.x) == 8) return V{1.0, 0.0};
+    else return V{0.0f, 0.0f};
+}
+// 32 well-mixed bits from a counter (an integer hash: xor-shift / multiply rounds).
+__device__ __forceinline__ uint32_t mix32(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    h *= 0x846ca68bu;
+    h ^= h >> 16;
+    return h;
+}
+
+// A uniform dither in [-1/2, 1/2) units in the last place of t (16 random bits); 0 for |t| below
+// 2^-102, where it no longer matters.
+__device__ __forceinline__ float dither_ulp(float t, uint32_t r16) {
+    // branch-free (a select), so that the table loads around it stay batched
+    const uint32_t eb = __float_as_uint(t) & 0x7f800000u;
+    const float ulp = __uint_as_float(eb > (24u << 23) ? eb - (23u << 23) : 0u);
+    return (float(r16) * (1.0f / 65536.0f) - 0.5f) * ulp;
+}
+
+// FP32 x (1 + d) with the second-order parts (x d_re: for a rotation by a small angle a,
+// d_re = cos a - 1 ~ -a^2/2) added under a dither of one unit in the last place. A rotation by an
+// angle below ~3e-4 changes the magnitude by less than half a unit in the last place, so nearest
+// rounding would drop that change at every application; the dithered sum keeps it on average (an
+// unbiased rounding), leaving a zero-mean error in place of a systematic drift of the norm.
+__device__ __forceinline__ float2 fmul_dither(float2 x, float2 d, uint32_t h) {
+    const float tr = fmaf(-x.y, d.y, x.x);
+    const float ti = fmaf(x.x, d.y, x.y);
+    return float2{tr + fmaf(x.x, d.x, dither_ulp(tr, h & 0xffffu)), ti + fmaf(x.y, d.x, dither_ulp(ti, h >> 16))};
+}
+
+// Multiply by a stored spectral factor of an axis of length L. In FP32 the entries of the lowest
+// momenta (|k| < L/E, `low`; after unrolling a compile-time choice) take the dithered product:
+// their spectral phases, which dominate a smooth state, are rotations by angles below 3e-4 for the
+// usual time steps. `key` identifies the element and the call.
+template <int L, typename V> __device__ __forceinline__ V fmul_spec(V x, V f, uint32_t key, bool low) {
+    if constexpr (sizeof(x.x) == 8) {
+        return cmul(x, f);
+    } else {
+        return cscale(low ? fmul_dither(x, f, mix32(key)) : fmul(x, f), 1.0f / float(L));
+    }
+}
+
 __host__ __device__ constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n >> 1); }
 
 // Correctly rounded cos(k*pi/16), k = 0..8 (exact mathematical constants; sin(k*pi/16) = cos((8-k)*pi/16)).
@@ -177,7 +245,7 @@ __device__ __forceinline__ void fft_stage_regs(V* v, int tid, const V* __restric
                 if constexpr (TWS) w = t[r - 1];
                 else w = __ldg(t + r - 1);
                 if constexpr (SIGN > 0) w.y = -w.y;
-                u[r] = cmul(u[r], w);
+                u[r] = fmul(u[r], w);
             }
         }
         RegDFT<R, SIGN>::run(u);

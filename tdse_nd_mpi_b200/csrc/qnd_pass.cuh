@@ -82,6 +82,7 @@ template <typename R> struct PassArgs {
                                  // (0); real factors (the step mask) always after the inverse
     R scale;
     int apply_acc;
+    unsigned seed;               // FP32: the random stream of the stochastic rounding (one per launch)
     const double* apply_vtab;
     RedDesc red;
 };
@@ -288,9 +289,10 @@ template <typename R, int E, int T>
 __device__ __forceinline__ void apply_factors(cplx_t<R>* v, int tid, long long base, long long lbase,
                                               const R* __restrict__ tr, const cplx_t<R>* __restrict__ tc,
                                               const cplx_t<R>* const* axc, const R* const* axr, int axis, int dim,
-                                              const int* shift, const long long* nmask, const double* scale_dev) {
+                                              const int* shift, const long long* nmask, const double* scale_dev,
+                                              uint32_t key) {
     using V = cplx_t<R>;
-    V lf = V{R(1), R(0)};
+    V lf = fone<V>();
     R lr = R(1);
     bool use_lf = false, use_lr = false;
     const V* __restrict__ pc = axc ? axc[axis] : nullptr;
@@ -299,21 +301,59 @@ __device__ __forceinline__ void apply_factors(cplx_t<R>* v, int tid, long long b
     for (int k = 0; k < MAX_DIM; ++k) {
         if (k >= dim || k == axis) continue;
         const long long ik = (base >> shift[k]) & nmask[k];
-        if (axc && axc[k]) { lf = cmul(lf, axc[k][ik]); use_lf = true; }
+        if (axc && axc[k]) { lf = fcompose(lf, axc[k][ik]); use_lf = true; }
         if (axr && axr[k]) { lr *= axr[k][ik]; use_lr = true; }
     }
     if (scale_dev) { lr *= R(*scale_dev); use_lr = true; }
+    if constexpr (sizeof(R) == 8) {
 #pragma unroll
-    for (int u = 0; u < E; ++u) {
-        const int m = tid + u * T;
-        V x = v[u];
-        if (tr) x = cscale(x, tr[lbase + m]);
-        if (tc) x = cmul(x, tc[lbase + m]);
-        if (pc) x = cmul(x, __ldg(pc + m));
-        if (pr) x = cscale(x, __ldg(pr + m));
-        if (use_lf) x = cmul(x, lf);
-        if (use_lr) x = cscale(x, lr);
-        v[u] = x;
+        for (int u = 0; u < E; ++u) {
+            const int m = tid + u * T;
+            V x = v[u];
+            if (tr) x = cscale(x, tr[lbase + m]);
+            if (tc) x = fmul(x, tc[lbase + m]);
+            if (pc) x = fmul(x, __ldg(pc + m));
+            if (pr) x = cscale(x, __ldg(pr + m));
+            if (use_lf) x = fmul(x, lf);
+            if (use_lr) x = cscale(x, lr);
+            v[u] = x;
+        }
+    } else {
+        // FP32: the per-axis laser phases near the origin, where the state lives, are rotations by
+        // angles ~1e-4 and take the dithered product (fmul_dither): along the pass axis the elements
+        // around the axis centre (u = E/2 - 1, E/2; a compile-time choice after unrolling), and the
+        // whole line when the factor of the other axes is a small rotation (a line-uniform branch).
+        // The potential tables rotate by h V, far from small where the state is.
+        const bool lf_small = use_lf && lf.y != 0.0f && fabsf(lf.y) < 2e-3f;
+        if (lf_small) {
+#pragma unroll
+            for (int u = 0; u < E; ++u) {
+                const int m = tid + u * T;
+                V x = v[u];
+                if (tr) x = cscale(x, tr[lbase + m]);
+                if (tc) x = fmul(x, tc[lbase + m]);
+                if (pc) x = (u == E / 2 - 1 || u == E / 2) ? fmul_dither(x, __ldg(pc + m), mix32(key + uint32_t(m)))
+                                                          : fmul(x, __ldg(pc + m));
+                if (pr) x = cscale(x, __ldg(pr + m));
+                x = fmul_dither(x, lf, mix32((key ^ 0x85ebca6bu) + uint32_t(m)));
+                if (use_lr) x = cscale(x, lr);
+                v[u] = x;
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < E; ++u) {
+                const int m = tid + u * T;
+                V x = v[u];
+                if (tr) x = cscale(x, tr[lbase + m]);
+                if (tc) x = fmul(x, tc[lbase + m]);
+                if (pc) x = (u == E / 2 - 1 || u == E / 2) ? fmul_dither(x, __ldg(pc + m), mix32(key + uint32_t(m)))
+                                                          : fmul(x, __ldg(pc + m));
+                if (pr) x = cscale(x, __ldg(pr + m));
+                if (use_lf) x = fmul(x, lf);
+                if (use_lr) x = cscale(x, lr);
+                v[u] = x;
+            }
+        }
     }
 }
 
@@ -343,6 +383,8 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
     const bool active = lam < nlines;
     const long long base = line_base(active ? lam : 0);
     const long long lbase = (active ? lam : 0) * L;  // line-major table offset of this line
+    // stochastic-rounding stream of this line: two spectral multiplies of L elements per line
+    const uint32_t key0 = mix32(a.seed) + uint32_t(lbase) * 2u;
 
     const V* tw = a.tw;
     if constexpr (TWS) {
@@ -390,7 +432,7 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
     if constexpr (PROPAGATE) {
         if (active && (a.pro_real || a.pro_cplx || a.pro_scale_dev || a.ax_in_prologue))
             apply_factors<R, E, T>(v, tid, base, lbase, a.pro_real, a.pro_cplx, a.ax_in_prologue ? a.ax_cplx : nullptr,
-                                   nullptr, a.axis, a.dim, a.shift, a.nmask, a.pro_scale_dev);
+                                   nullptr, a.axis, a.dim, a.shift, a.nmask, a.pro_scale_dev, key0 ^ 0x51ed270bu);
     }
     if constexpr (STRIDED) lsync();  // staged inputs read before the exchanges reuse the buffer
 
@@ -416,14 +458,15 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
         if (a.spec) {
             const V* __restrict__ sp = a.spec;
 #pragma unroll
-            for (int u = 0; u < E; ++u) v[u] = cmul(v[u], __ldg(sp + tid + u * T));
+            for (int u = 0; u < E; ++u)
+                v[u] = fmul_spec<L>(v[u], __ldg(sp + tid + u * T), key0 + uint32_t(tid + u * T), u == 0 || u == E - 1);
         }
         fft_line_stages<L, E, +1, 0, TWS>(v, tid, line, tw, lsync);
         if constexpr (MODE == PM_DOUBLE) {
             // r-space factor between the two sandwiches, then the second sandwich on the same axis
             if (active) {
                 apply_factors<R, E, T>(v, tid, base, lbase, a.mid_real, a.mid_cplx, a.mid_ax_cplx, a.mid_ax_real,
-                                       a.axis, a.dim, a.shift, a.nmask, nullptr);
+                                       a.axis, a.dim, a.shift, a.nmask, nullptr, key0 ^ 0x2545f491u);
                 // a step boundary inside the pass: observables of the state between the two steps
                 if (a.red_at_mid && a.red.n)
                     accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);
@@ -434,7 +477,9 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
             if (a.spec2) {
                 const V* __restrict__ sp2 = a.spec2;
 #pragma unroll
-                for (int u = 0; u < E; ++u) v[u] = cmul(v[u], __ldg(sp2 + tid + u * T));
+                for (int u = 0; u < E; ++u)
+                    v[u] = fmul_spec<L>(v[u], __ldg(sp2 + tid + u * T), key0 + uint32_t(L + tid + u * T),
+                                        u == 0 || u == E - 1);
             }
             fft_line_stages<L, E, +1, 0, TWS>(v, tid, line, tw, lsync);
         }
@@ -443,10 +488,10 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
                 if (a.epi_real || a.epi_cplx || !a.ax_in_prologue)
                     apply_factors<R, E, T>(v, tid, base, lbase, a.epi_real, a.epi_cplx,
                                            a.ax_in_prologue ? nullptr : a.ax_cplx, a.ax_real, a.axis, a.dim, a.shift,
-                                           a.nmask, nullptr);
+                                           a.nmask, nullptr, key0 ^ 0x68e31da4u);
                 else
                     apply_factors<R, E, T>(v, tid, base, lbase, nullptr, nullptr, nullptr, a.ax_real, a.axis, a.dim,
-                                           a.shift, a.nmask, nullptr);
+                                           a.shift, a.nmask, nullptr, key0 ^ 0x68e31da4u);
                 if (a.red.n && !a.red_at_mid)
                     accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);
             } else {  // PM_APPLY

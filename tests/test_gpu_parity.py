@@ -355,3 +355,28 @@ def test_multistep_length_velocity_imag_vs_oracle(Grid, shape, dr):
     st.upload(psi0)
     grid.integration_step_imag(st, n)
     assert rel(st.download(), a) < TOL
+
+
+def test_graph_replayed_chunks_match_direct_launches(Grid, monkeypatch):
+    """Runs longer than one chunk (128 steps): the first chunk runs directly, the second is
+    captured into a CUDA graph and the later ones replay it. Same results as direct launches
+    (QND_NO_GRAPH) and as the oracle."""
+    shape, dr = (64, 128), (0.4, 0.3)
+    grid, o = _masked_pair(Grid, shape, dr)
+    psi0 = O.smooth_state(shape, dr, 14)
+    nsteps = 300
+    E = np.random.default_rng(15).standard_normal((nsteps, grid.s, 2)) * 0.05
+    names = ["norm", "dipole_r", "accel"]
+    st = grid.state(psi0)
+    ob_graph = grid.run_length(st, E, names)
+    psi_graph = st.download()
+    monkeypatch.setenv("QND_NO_GRAPH", "1")
+    st.upload(psi0)
+    ob_direct = grid.run_length(st, E, names)
+    np.testing.assert_array_equal(ob_graph, ob_direct)
+    np.testing.assert_array_equal(psi_graph, st.download())
+    monkeypatch.delenv("QND_NO_GRAPH")
+    a = psi0.copy()
+    ob_o = o.run_length(a, E, names)
+    assert rel(psi_graph, a) < 1e-11
+    np.testing.assert_allclose(ob_graph, ob_o, rtol=1e-10, atol=1e-13)
