@@ -130,6 +130,19 @@ int qnd_observables(qnd_ctx *ctx, const void *psi_r_dev, int nobs, const char *c
 /* Calculation_global_energies (calculate_observables.c:89-116): out[m] = Re <psi|H^(m+1)|psi> dNr. */
 int qnd_energies(qnd_ctx *ctx, const void *psi_r_dev, int n, double *out_host);
 
+/* ---- final photoelectron spectra: Write_final_observables (io_functions.c:136-287) on the device.
+ * psi_r_dev (not modified) is multiplied by the radial mask of R_MASK (sin^2 between r_mask_min and
+ * r_mask_max, 1 beyond; io_functions.c:159-167) and taken to the unitary p-representation.
+ *  - npr_host[dim] (may be NULL) receives the kept momenta per axis, |p_j| <= pr_max[j] (the NPR
+ *    header of PMD.real).
+ *  - ped_host[ne] (may be NULL): the energy distribution S(j de), Gaussian width de, over the kept
+ *    momenta (io_functions.c:192-199; the rows of PED.real are j*de, ped_host[j]).
+ *  - pmd_host[2 * prod(npr)] (may be NULL): (|psi~|^2, arg psi~) of the kept momenta in flat FFT
+ *    order, the binary block of PMD.real (io_functions.c:266-274).
+ * Call with both NULL to get the counts first. Synchronises. */
+int qnd_final_spectra(qnd_ctx *ctx, const void *psi_r_dev, double r_mask_min, double r_mask_max, const double *pr_max,
+                      double de, int ne, double *ped_host, int64_t *npr_host, double *pmd_host);
+
 /* ---- r-space observables without allocation (no reference counterpart).
  * Computes the "norm", "dipole_r" and "accel" values of qnd_observables, in the same row layout,
  * with the same reduction, into the caller's device buffer out_dev[nvalues]. It is asynchronous

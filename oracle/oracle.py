@@ -142,6 +142,8 @@ def ref_lib(fast: bool = False):
         L.ref_run_length.argtypes = [_vp, _vp, _dp, _ll, C.c_int, C.POINTER(C.c_char_p), _dp]
         L.ref_run_velocity.argtypes = [_vp, _vp, _dp, _dp, _ll, C.c_int, C.POINTER(C.c_char_p), _dp]
         L.ref_to_p.argtypes = [_vp, _vp]
+        L.ref_final_observables.argtypes = [_vp, _vp, C.c_double, C.c_double, _dp, C.c_double, C.c_int, C.c_int,
+                                            C.POINTER(C.c_char_p)]
         L.ref_to_r.argtypes = [_vp, _vp]
         L.ref_field.restype = _ll
         L.ref_field.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_char_p), C.c_char_p,
@@ -450,6 +452,80 @@ class RefCtx(_Base):
         self.L.ref_run_velocity(self.h, _ptr(self._check(psi_r)), _dptr(A), _dptr(al), nsteps, len(names),
                                 _cstrs(names), _dptr(out))
         return out[:, :nv]
+
+    def final_observables(self, psi_r, r_mask, pr_max, de, ne, names=("PED", "PMD")):
+        """Write_final_observables (io_functions.c:136-287) run in a scratch directory; returns the
+        files it wrote as {"PED": [ne, 2] array, "PMD": (header dict, [count, 2] array)}."""
+        import tempfile
+
+        psi = self._check(psi_r.copy())
+        prm = _f64(pr_max)
+        out = {}
+        cwd = os.getcwd()
+        with tempfile.TemporaryDirectory() as tmp:
+            os.chdir(tmp)
+            try:
+                self.L.ref_final_observables(self.h, _ptr(psi), float(r_mask[0]), float(r_mask[1]), _dptr(prm),
+                                             float(de), int(ne), len(names), _cstrs(list(names)))
+                if os.path.exists("PED.real"):
+                    out["PED"] = np.loadtxt("PED.real").reshape(-1, 2)
+                if os.path.exists("PMD.real"):
+                    out["PMD"] = read_pmd("PMD.real")
+            finally:
+                os.chdir(cwd)
+        return out
+
+
+def grid_axes(shape, dr):
+    """r axes (-L/2 + i dr) and p axes in FFT order (meshgrid.c:75-89)."""
+    rs, ps = [], []
+    for n, d in zip(shape, dr):
+        rs.append(-0.5 * n * d + np.arange(n) * d)
+        dp = 2.0 * np.pi / (n * d)
+        k = np.arange(n)
+        ps.append(np.where(k < n // 2, k, k - n) * dp)
+    return rs, ps
+
+
+def final_spectra_numpy(psi_r, dr, r_mask, pr_max, de, ne):
+    """Restatement of Write_final_observables (io_functions.c:136-287) for the checks: the sin^2
+    R_MASK mask, the unitary forward FFT (numpy's sign convention is FFTW's forward), the PED over
+    the momenta with every |p_j| <= pr_max_j, and the packed PMD (|psi~|^2, arg psi~)."""
+    shape = psi_r.shape
+    dim = len(shape)
+    rs, ps = grid_axes(shape, dr)
+    R = np.sqrt(sum(x * x for x in np.meshgrid(*rs, indexing="ij")))
+    f = np.where(R > r_mask[1], 1.0, 0.0)
+    zone = (R >= r_mask[0]) & (R <= r_mask[1])
+    f[zone] = np.sin(0.5 * np.pi * (R[zone] - r_mask[0]) / (r_mask[1] - r_mask[0])) ** 2
+    q = np.fft.fftn(f * psi_r) / np.sqrt(psi_r.size)
+    P = np.meshgrid(*ps, indexing="ij")
+    kin = sum(0.5 * p * p for p in P)
+    keep_ax = [np.abs(p) <= m for p, m in zip(ps, pr_max)]
+    keep = np.ones(shape, dtype=bool)
+    for j, k in enumerate(keep_ax):
+        sl = [None] * dim
+        sl[j] = slice(None)
+        keep &= k[tuple(sl)]
+    w = np.abs(q[keep]) ** 2
+    E = np.arange(ne) * de
+    norm = 1.0 / (2.0 * np.pi * de * de) ** (0.5 * dim)
+    ped = np.array([np.sum(w * np.exp(-0.5 * (kin[keep] - e) ** 2 / (de * de))) * norm for e in E])
+    pmd = np.stack([np.abs(q[keep]) ** 2, np.angle(q[keep])], axis=1)
+    return ped, [int(k.sum()) for k in keep_ax], pmd
+
+
+def read_pmd(path):
+    """PMD.real (io_functions.c:236-281): text header, DATA_START, then (|psi~|^2, arg) doubles."""
+    raw = open(path, "rb").read()
+    k = raw.index(b"DATA_START\n") + len(b"DATA_START\n")
+    head = {}
+    for line in raw[:k].decode().splitlines():
+        parts = line.split("\t")
+        if parts[0] in ("NPR", "DP", "DIMENSION"):
+            head[parts[0]] = [float(x) for x in parts[1:]]
+    data = np.frombuffer(raw[k:], dtype=np.float64).reshape(-1, 2)
+    return head, data
 
 
 def seeded_state(shape, seed, normalise_dnr=None):

@@ -13,6 +13,7 @@
  *   Gram_Schmidt_orthonormalization  QuantumND_imag.c:265-311
  *   Calculation_global_energies / _observables  calculate_observables.c:89-140
  *   Field_vectors                parameters.c:899-949
+ *   Write_final_observables      io_functions.c:136-287
  * The driver loops (QuantumND_imag.c:182-185, QuantumND_real.c:168-229) are
  * replayed here call for call so trajectories match the executables.
  */
@@ -24,6 +25,7 @@
 
 #include "calculate_observables.h"
 #include "integrators.h"
+#include "io_functions.h"
 #include "meshgrid.h"
 #include "parameters.h"
 
@@ -291,4 +293,23 @@ void ref_field_at(int dim, int nmodes, const double *intensity, const double *la
     Field_vectors(&P, &F, t, A, E, MPI_COMM_WORLD);
     free(F.amplitude);
     free(F.frequency);
+}
+
+/*
+ * Write_final_observables (io_functions.c:136-287) on psi (r-space; masked and transformed in
+ * place, as the reference does at the end of QuantumND_real): writes PED.real, PMD.real and
+ * wavefunction.real into the current directory.
+ */
+void ref_final_observables(RefCtx *c, double complex *psi, double rmin, double rmax, const double *pr_max, double de,
+                           int ne, int nobs, char **names) {
+    for (int j = 0; j < c->P.dim; ++j) c->P.pr_max[j] = pr_max[j];
+    c->P.R_mask[0] = rmin;
+    c->P.R_mask[1] = rmax;
+    c->P.de = de;
+    c->P.Ne = ne;
+    Observables Obs;
+    memset(&Obs, 0, sizeof Obs);
+    Initialize_observables(&Obs, names, nobs, c->P.dim, MPI_COMM_WORLD);
+    Write_final_observables(psi, &c->P, &c->grid, &Obs, c->local_start, MPI_COMM_WORLD);
+    Finalize_observables(&Obs);
 }

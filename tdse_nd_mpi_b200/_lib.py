@@ -54,6 +54,7 @@ SIGNATURES = {
     "qnd_observables": ([_vp, _vp, C.c_int, _names, _dp, _dp], C.c_int),
     "qnd_energies": ([_vp, _vp, C.c_int, _dp], C.c_int),
     "qnd_observables_rspace_noalloc": ([_vp, _vp, C.c_int, _names, _vp], C.c_int),
+    "qnd_final_spectra": ([_vp, _vp, C.c_double, C.c_double, _dp, C.c_double, C.c_int, _dp, _i64p, _dp], C.c_int),
 }
 
 _lib = None

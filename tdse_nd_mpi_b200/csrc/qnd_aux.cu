@@ -144,13 +144,133 @@ template <typename R> void launch_axis_table(int mode, const double* p, int N, d
     axis_table_kernel<R><<<(N + 255) / 256, 256, 0, st>>>(mode, p, N, alpha, out);
 }
 
+// ---- final photoelectron spectra (io_functions.c:136-287) -------------------------
+
+// out = f(|r|) in, f = sin^2(pi/2 (|r| - rmin)/(rmax - rmin)) between rmin and rmax, 1 beyond, 0 inside
+// (io_functions.c:159-167).
+template <typename R>
+__global__ void __launch_bounds__(256) radial_mask_kernel(const __grid_constant__ SpectraArgs a, const cplx_t<R>* in,
+                                                          cplx_t<R>* out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (long long)gridDim.x * blockDim.x) {
+        double r2 = 0.0;
+        for (int j = 0; j < a.dim; ++j) {
+            const double x = a.r[a.axoff[j] + ((i >> a.shift[j]) & a.nmask[j])];
+            r2 += x * x;
+        }
+        const double radius = sqrt(r2);
+        double f = 0.0;
+        if (radius >= a.rmin && radius <= a.rmax) {
+            const double sn = sin(0.5 * 3.14159265358979323846 * (radius - a.rmin) / (a.rmax - a.rmin));
+            f = sn * sn;
+        } else if (radius > a.rmax) {
+            f = 1.0;
+        }
+        const cplx_t<R> v = in[i];
+        out[i] = cplx_t<R>{R(double(v.x) * f), R(double(v.y) * f)};
+    }
+}
+
+// Energy distribution: block b sums, for every energy bin, the Gaussian-weighted densities of its
+// PED_CHUNK elements (those with every |p_j| <= pr_max_j); a second kernel adds the blocks' partial
+// sums in block order (deterministic) and applies the normalisation (io_functions.c:192-199). Bins
+// further than 39 sigma from an element's kinetic energy get exp(...) < 1e-330, which is zero.
+template <typename R>
+__global__ void __launch_bounds__(256) ped_partial_kernel(const __grid_constant__ SpectraArgs a, const cplx_t<R>* psi,
+                                                          double* partials) {
+    __shared__ double w_s[PED_CHUNK], k_s[PED_CHUNK];
+    const long long i0 = (long long)blockIdx.x * PED_CHUNK;
+    for (int c = threadIdx.x; c < PED_CHUNK; c += blockDim.x) {
+        const long long i = i0 + c;
+        double w = 0.0, kin = 0.0;
+        if (i < a.n) {
+            bool keep = true;
+            for (int j = 0; j < a.dim; ++j) {
+                const long long ij = (i >> a.shift[j]) & a.nmask[j];
+                if (a.rank[a.axoff[j] + ij] < 0) keep = false;
+                const double pj = a.p[a.axoff[j] + ij];
+                kin += .5 * pj * pj;
+            }
+            if (keep) {
+                const cplx_t<R> v = psi[i];
+                const double m = sqrt(double(v.x) * double(v.x) + double(v.y) * double(v.y));
+                w = m * m;
+            }
+        }
+        w_s[c] = w;
+        k_s[c] = kin;
+    }
+    __syncthreads();
+    const double inv2s2 = .5 / (a.sigma * a.sigma), reach = 39.0 * a.sigma;
+    for (int j = threadIdx.x; j < a.ne; j += blockDim.x) {
+        const double e = j * a.de;
+        double s = 0.0;
+        for (int c = 0; c < PED_CHUNK; ++c) {
+            const double d = k_s[c] - e;
+            if (w_s[c] != 0.0 && fabs(d) <= reach) s += w_s[c] * exp(-d * d * inv2s2);
+        }
+        partials[(long long)blockIdx.x * a.ne + j] = s;
+    }
+}
+
+__global__ void ped_final_kernel(const __grid_constant__ SpectraArgs a, const double* partials, int nblocks, double* out) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < a.ne; j += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; ++b) s += partials[(long long)b * a.ne + j];
+        out[j] = s * a.norm;
+    }
+}
+
+// Momentum distribution: (|psi~|^2, arg psi~) of the kept momenta, packed in flat order
+// (io_functions.c:266-274); the kept set is a product of per-axis sets, so an element's place in the
+// packed array follows from its per-axis ranks.
+template <typename R>
+__global__ void __launch_bounds__(256) pmd_kernel(const __grid_constant__ SpectraArgs a, const cplx_t<R>* psi,
+                                                  double* out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (long long)gridDim.x * blockDim.x) {
+        long long q = 0;
+        bool keep = true;
+        for (int j = 0; j < a.dim; ++j) {
+            const int rk = a.rank[a.axoff[j] + ((i >> a.shift[j]) & a.nmask[j])];
+            if (rk < 0) keep = false;
+            q += (long long)rk * a.stride[j];
+        }
+        if (!keep) continue;
+        const cplx_t<R> v = psi[i];
+        const double re = v.x, im = v.y;
+        const double m = sqrt(re * re + im * im);
+        out[2 * q] = m * m;
+        out[2 * q + 1] = atan2(im, re);
+    }
+}
+
+template <typename R>
+void launch_radial_mask(const SpectraArgs& a, const cplx_t<R>* in, cplx_t<R>* out, cudaStream_t st) {
+    long long nb = (a.n + 255) / 256;
+    if (nb > 148 * 16) nb = 148 * 16;
+    radial_mask_kernel<R><<<(int)nb, 256, 0, st>>>(a, in, out);
+}
+template <typename R>
+void launch_ped(const SpectraArgs& a, const cplx_t<R>* psi_p, double* partials, double* out, cudaStream_t st) {
+    const int nb = int((a.n + PED_CHUNK - 1) / PED_CHUNK);
+    ped_partial_kernel<R><<<nb, 256, 0, st>>>(a, psi_p, partials);
+    ped_final_kernel<<<(a.ne + 255) / 256, 256, 0, st>>>(a, partials, nb, out);
+}
+template <typename R> void launch_pmd(const SpectraArgs& a, const cplx_t<R>* psi_p, double* out, cudaStream_t st) {
+    long long nb = (a.n + 255) / 256;
+    if (nb > 148 * 16) nb = 148 * 16;
+    pmd_kernel<R><<<(int)nb, 256, 0, st>>>(a, psi_p, out);
+}
+
 #define QND_INST(R)                                                                               \
     template void launch_gs_dot<R>(const GSArgs<R>&, cudaStream_t, int);                          \
     template void launch_gs_axpy<R>(const GSArgs<R>&, cudaStream_t, int);                         \
     template void launch_grid_reduce<R>(const PassArgs<R>&, long long, cudaStream_t, int);        \
     template void launch_scale<R>(cplx_t<R>*, long long, const double*, cudaStream_t);            \
     template void launch_field_tables<R>(const FieldTableArgs&, cplx_t<R>*, cudaStream_t);        \
-    template void launch_axis_table<R>(int, const double*, int, double, void*, cudaStream_t);
+    template void launch_axis_table<R>(int, const double*, int, double, void*, cudaStream_t);             \
+    template void launch_radial_mask<R>(const SpectraArgs&, const cplx_t<R>*, cplx_t<R>*, cudaStream_t);  \
+    template void launch_ped<R>(const SpectraArgs&, const cplx_t<R>*, double*, double*, cudaStream_t);    \
+    template void launch_pmd<R>(const SpectraArgs&, const cplx_t<R>*, double*, cudaStream_t);
 QND_INST(double)
 QND_INST(float)
 #undef QND_INST

@@ -148,6 +148,7 @@ struct qnd_ctx {
     DevBuf gs_flag;
     DevBuf field_dev, field_tab, wtab_dev[MAX_DIM], spec_tmp[MAX_DIM];
     DevBuf scratch_a, scratch_b;
+    DevBuf spec_rank, spec_partials, spec_out;  // final spectra: per-axis ranks, partial sums, results
     std::vector<char> host_tmp;
 
     int num_sms = 148;
@@ -1999,6 +2000,92 @@ int qnd_energies(qnd_ctx* ctx, const void* psi_r_dev, int n, double* out_host) {
     energy_moments(ctx, psi_r_dev, n, ctx->obs_dev.as<double>());
     QND_CK(cudaMemcpyAsync(out_host, ctx->obs_dev.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     QND_CK(cudaStreamSynchronize(ctx->stream));
+    QND_API_END
+}
+
+int qnd_final_spectra(qnd_ctx* ctx, const void* psi_r_dev, double r_mask_min, double r_mask_max, const double* pr_max,
+                      double de, int ne, double* ped_host, int64_t* npr_host, double* pmd_host) {
+    using namespace qnd;
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_r_dev);
+    QND_NEED(pr_max);
+    if (ped_host && (ne <= 0 || !(de > 0.0))) QND_FAIL(QND_EINVAL, "qnd_final_spectra: the PED needs NE > 0 and DE > 0");
+    if (!(r_mask_max > r_mask_min)) QND_FAIL(QND_EINVAL, "qnd_final_spectra: R_MASK needs Rmin < Rmax");
+    set_device(ctx);
+    const int d = ctx->dim;
+    // kept momenta per axis (|p| <= pr_max, io_functions.c:191, :218-225) and their ranks
+    std::vector<int> rank(size_t(ctx->axtot), -1);
+    int64_t npr[MAX_DIM] = {0, 0, 0};
+    for (int j = 0; j < d; ++j)
+        for (int k = 0; k < int(ctx->nr[j]); ++k)
+            if (std::fabs(ctx->p[j][k]) <= pr_max[j]) rank[ctx->axoff[j] + k] = int(npr[j]++);
+    if (npr_host)
+        for (int j = 0; j < d; ++j) npr_host[j] = npr[j];
+    if (!ped_host && !pmd_host) return QND_OK;
+    ctx->spec_rank.ensure(rank.size() * sizeof(int));
+    QND_CK(cudaMemcpyAsync(ctx->spec_rank.p, rank.data(), rank.size() * sizeof(int), cudaMemcpyHostToDevice,
+                           ctx->stream));
+    SpectraArgs a{};
+    a.r = ctx->r_dev.as<double>();
+    a.p = ctx->p_dev.as<double>();
+    a.rank = ctx->spec_rank.as<int>();
+    a.dim = d;
+    a.n = ctx->n;
+    long long stride = 1;
+    for (int j = d - 1; j >= 0; --j) {
+        a.stride[j] = stride;
+        stride *= npr[j];
+    }
+    for (int j = 0; j < d; ++j) {
+        a.axoff[j] = ctx->axoff[j];
+        a.shift[j] = ctx->shift[j];
+        a.nmask[j] = ctx->nr[j] - 1;
+    }
+    a.rmin = r_mask_min;
+    a.rmax = r_mask_max;
+    a.de = de;
+    a.sigma = de;
+    a.ne = ne;
+    a.norm = 1.0 / std::pow(2.0 * M_PI * de * de, .5 * d);
+    // the masked state, in the unitary p-representation (io_functions.c:158-170)
+    ensure_scratch_state(ctx, ctx->scratch_a);
+    void* q = ctx->scratch_a.p;
+    if (ctx->fp64)
+        launch_radial_mask<double>(a, static_cast<const double2*>(psi_r_dev), static_cast<double2*>(q), ctx->stream);
+    else
+        launch_radial_mask<float>(a, static_cast<const float2*>(psi_r_dev), static_cast<float2*>(q), ctx->stream);
+    ctx->kernels_launched++;
+    QND_CK(cudaGetLastError());
+    unitary_fft(ctx, q, true);
+    if (ped_host) {
+        const size_t nb = size_t((ctx->n + PED_CHUNK - 1) / PED_CHUNK);
+        ctx->spec_partials.ensure(nb * size_t(ne) * sizeof(double));
+        ctx->spec_out.ensure(size_t(ne) * sizeof(double));
+        if (ctx->fp64)
+            launch_ped<double>(a, static_cast<const double2*>(q), ctx->spec_partials.as<double>(),
+                               ctx->spec_out.as<double>(), ctx->stream);
+        else
+            launch_ped<float>(a, static_cast<const float2*>(q), ctx->spec_partials.as<double>(),
+                              ctx->spec_out.as<double>(), ctx->stream);
+        ctx->kernels_launched += 2;
+        QND_CK(cudaGetLastError());
+        QND_CK(cudaMemcpyAsync(ped_host, ctx->spec_out.p, size_t(ne) * sizeof(double), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+        QND_CK(cudaStreamSynchronize(ctx->stream));
+    }
+    if (pmd_host && stride > 0) {
+        ctx->spec_out.ensure(size_t(stride) * 2 * sizeof(double));
+        if (ctx->fp64)
+            launch_pmd<double>(a, static_cast<const double2*>(q), ctx->spec_out.as<double>(), ctx->stream);
+        else
+            launch_pmd<float>(a, static_cast<const float2*>(q), ctx->spec_out.as<double>(), ctx->stream);
+        ctx->kernels_launched++;
+        QND_CK(cudaGetLastError());
+        QND_CK(cudaMemcpyAsync(pmd_host, ctx->spec_out.p, size_t(stride) * 2 * sizeof(double), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+        QND_CK(cudaStreamSynchronize(ctx->stream));
+    }
     QND_API_END
 }
 

@@ -78,4 +78,26 @@ template <typename R> void launch_field_tables(const FieldTableArgs& a, cplx_t<R
 //   mode 1: spec[k] = (p[k] + alpha) / N (complex)   Lz operator
 template <typename R> void launch_axis_table(int mode, const double* p, int N, double alpha, void* out, cudaStream_t st);
 
+// Final photoelectron spectra (Write_final_observables, io_functions.c:136-287).
+struct SpectraArgs {
+    const double* r;      // concatenated r axes
+    const double* p;      // concatenated p axes (FFT order)
+    const int* rank;      // concatenated per-axis rank among the kept momenta (|p| <= pr_max), -1 if not kept
+    int axoff[MAX_DIM];
+    int shift[MAX_DIM];
+    long long nmask[MAX_DIM];
+    long long stride[MAX_DIM];  // strides of the packed PMD array
+    int dim;
+    long long n;
+    double rmin, rmax;    // sin^2 mask between rmin and rmax, 1 beyond (R_MASK)
+    double de, sigma, norm;
+    int ne;
+};
+constexpr int PED_CHUNK = 256;  // elements per block of the energy-distribution partial sums
+template <typename R>
+void launch_radial_mask(const SpectraArgs& a, const cplx_t<R>* in, cplx_t<R>* out, cudaStream_t st);
+template <typename R>
+void launch_ped(const SpectraArgs& a, const cplx_t<R>* psi_p, double* partials, double* out, cudaStream_t st);
+template <typename R> void launch_pmd(const SpectraArgs& a, const cplx_t<R>* psi_p, double* out, cudaStream_t st);
+
 }  // namespace qnd

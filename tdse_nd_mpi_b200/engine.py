@@ -286,6 +286,20 @@ class Grid:
                                     _dptr(out)))
         return out[:nv]
 
+    def final_spectra(self, psi_r, r_mask, pr_max, de, ne):
+        """Write_final_observables (io_functions.c:136-287) on the device: returns (ped [ne], npr [dim],
+        pmd [prod(npr), 2]) for the R_MASK r_mask, momentum limits pr_max and the PED grid j*de."""
+        prm = _f64(np.broadcast_to(np.asarray(pr_max, dtype=np.float64), (self.dim,)).copy())
+        npr = (C.c_int64 * self.dim)()
+        check(lib().qnd_final_spectra(self.h, C.c_void_p(_ptr_of(psi_r)), float(r_mask[0]), float(r_mask[1]),
+                                      _dptr(prm), float(de), int(ne), None, npr, None))
+        counts = [int(v) for v in npr]
+        ped = np.zeros(max(int(ne), 1))
+        pmd = np.zeros((int(np.prod(counts)), 2))
+        check(lib().qnd_final_spectra(self.h, C.c_void_p(_ptr_of(psi_r)), float(r_mask[0]), float(r_mask[1]),
+                                      _dptr(prm), float(de), int(ne), _dptr(ped), npr, _dptr(pmd)))
+        return ped[:int(ne)], counts, pmd
+
     def energies(self, psi_r, n=2):
         out = np.zeros(n)
         check(lib().qnd_energies(self.h, C.c_void_p(_ptr_of(psi_r)), int(n), _dptr(out)))

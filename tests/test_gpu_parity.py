@@ -380,3 +380,32 @@ def test_graph_replayed_chunks_match_direct_launches(Grid, monkeypatch):
     ob_o = o.run_length(a, E, names)
     assert rel(psi_graph, a) < 1e-11
     np.testing.assert_allclose(ob_graph, ob_o, rtol=1e-10, atol=1e-13)
+
+
+@pytest.mark.parametrize("shape,dr,pot,rmask,prmax", [((512,), (0.2,), "H_1D", (10.0, 20.0), (3.0,)),
+                                                      ((64, 64), (0.3, 0.3), "H_2D", (3.0, 8.0), (4.0, 2.5)),
+                                                      ((16, 16, 32), (0.5, 0.5, 0.4), "H_3D", (2.0, 5.0), (3.0, 3.0, 5.0))])
+def test_final_spectra_vs_reference(Grid, shape, dr, pot, rmask, prmax):
+    """PED and PMD (Write_final_observables, io_functions.c:136-287) against the reference's own
+    function compiled from its sources: the energy distribution, the kept-momentum counts and the
+    packed (|psi~|^2, arg psi~) pairs."""
+    grid = Grid(len(shape), shape, dr, "BM4", 0.05)
+    grid.set_potential(pot)
+    psi = O.smooth_state(shape, dr, 16) * np.exp(1j * 0.7 * O.seeded_state(shape, 17).real)
+    de, ne = 0.02, 120
+    if O.ref_available():
+        out = O.RefCtx(len(shape), shape, dr, "BM4", 0.05, potential=pot).final_observables(psi, rmask, prmax, de, ne)
+    else:  # the restatement, pinned to the reference by test_oracle
+        p_, c_, d_ = O.final_spectra_numpy(psi, dr, rmask, prmax, de, ne)
+        out = {"PED": np.stack([np.arange(ne) * de, p_], axis=1), "PMD": ({"NPR": c_}, d_)}
+    ped, counts, pmd = grid.final_spectra(grid.state(psi), rmask, prmax, de, ne)
+    np.testing.assert_allclose(out["PED"][:, 0], np.arange(ne) * de, rtol=0, atol=1e-15)
+    np.testing.assert_allclose(ped, out["PED"][:, 1], rtol=0, atol=1e-11 * np.max(np.abs(out["PED"][:, 1])))
+    head, data = out["PMD"]
+    assert counts == [int(v) for v in head["NPR"]]
+    assert pmd.shape == data.shape
+    dens = data[:, 0]
+    np.testing.assert_allclose(pmd[:, 0], dens, rtol=0, atol=1e-12 * dens.max())
+    live = dens > 1e-10 * dens.max()
+    dphi = np.angle(np.exp(1j * (pmd[live, 1] - data[live, 1])))
+    assert np.max(np.abs(dphi)) < 1e-8

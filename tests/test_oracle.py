@@ -174,3 +174,20 @@ def test_oracle_3d_and_1d_bit_identical_to_reference():
         a, b = psi.copy(), psi.copy()
         assert np.array_equal(o.run_length(a, E, names), r.run_length(b, E, names))
         assert np.array_equal(a, b)
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference not compiled here (needs its sources)")
+@pytest.mark.parametrize("shape,dr,pot", [((256,), (0.2,), "H_1D"), ((32, 64), (0.3, 0.25), "H_2D")])
+def test_final_spectra_restatement_matches_reference(shape, dr, pot):
+    """The PED/PMD restatement used by the checks against Write_final_observables itself."""
+    r = O.RefCtx(len(shape), shape, dr, "BM4", 0.05, potential=pot, nthreads=2)
+    psi = O.smooth_state(shape, dr, 4) * np.exp(0.5j * O.seeded_state(shape, 5).real)
+    rmask, prmax, de, ne = (2.0, 6.0), (3.0,) * len(shape), 0.03, 80
+    out = r.final_observables(psi, rmask, prmax, de, ne)
+    ped, counts, pmd = O.final_spectra_numpy(psi, dr, rmask, prmax, de, ne)
+    np.testing.assert_allclose(ped, out["PED"][:, 1], rtol=0, atol=1e-12 * out["PED"][:, 1].max())
+    head, data = out["PMD"]
+    assert counts == [int(v) for v in head["NPR"]]
+    np.testing.assert_allclose(pmd[:, 0], data[:, 0], rtol=0, atol=1e-13 * data[:, 0].max())
+    live = data[:, 0] > 1e-10 * data[:, 0].max()
+    assert np.max(np.abs(np.angle(np.exp(1j * (pmd[live, 1] - data[live, 1]))))) < 1e-9
