@@ -82,7 +82,30 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
         os.replace(tmp, LIB)
+    build_drivers(force)
     return LIB
+
+
+DRIVERS = {"QuantumND_imag": ["quantumnd_imag.c", "params.c"]}
+
+
+def build_drivers(force: bool = False) -> list[str]:
+    """The drop-in C drivers (drivers/*.c), linked against libqnd_b200.so next to them."""
+    cc = shutil.which("gcc") or "cc"
+    src_dir = os.path.join(PKG, "drivers")
+    out = []
+    for exe, srcs in DRIVERS.items():
+        target = os.path.join(PKG, exe)
+        paths = [os.path.join(src_dir, f) for f in srcs]
+        deps = paths + [os.path.join(src_dir, "params.h"), os.path.join(ROOT, "include", "qnd.h"), LIB]
+        if force or not os.path.exists(target) or os.path.getmtime(target) < max(os.path.getmtime(d) for d in deps):
+            cmd = [cc, "-O2", "-std=gnu11", "-I", os.path.join(ROOT, "include"), "-o", target] + paths + \
+                  ["-L", PKG, "-lqnd_b200", "-Wl,-rpath,$ORIGIN", "-lm"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"driver build failed ({exe}):\n{r.stderr}")
+        out.append(target)
+    return out
 
 
 if __name__ == "__main__":
