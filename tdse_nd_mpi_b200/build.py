@@ -86,7 +86,7 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
     return LIB
 
 
-DRIVERS = {"QuantumND_imag": ["quantumnd_imag.c", "params.c"]}
+DRIVERS = {"QuantumND_imag": ["quantumnd_imag.c", "params.c"], "QuantumND_real": ["quantumnd_real.c", "params.c"]}
 
 
 def build_drivers(force: bool = False) -> list[str]:

@@ -90,3 +90,97 @@ def test_output_imag_matches_reference_executable(driver, tmp_path):
     assert np.linalg.norm(psi1 - psi2) / np.linalg.norm(psi2) < 1e-10
     for line in ("PROGRAM IMAGINARY-TIME PROPAGATION", "> eigenfunction 3:", "# The code ended successfully"):
         assert line in r1.stdout
+
+
+REAL_DRIVER = os.path.join(ROOT, "tdse_nd_mpi_b200", "QuantumND_real")
+REF_REAL = os.path.join(ROOT, "oracle", "_ref", "QuantumND_real")
+
+PARAMS_REAL = """OUTPUT_IMAG\toutput.imag
+NR\t\t512
+N_STATES\t2
+J_STATES\t1 2
+COEFFS_STATES\t1. 0.5+0.5j
+CAP\t\t.1 20.
+GAUGE\t\t{gauge}
+N_MODES\t\t2
+INTENSITY\t1.e13 5.e12
+LAMBDA\t\t800 400
+ELLIPTICITY\t0. 0.
+CEP\t\t0. 1.
+DELAY\t\t0. 10.
+ENVELOPE\tcos2 trapz
+DURATION\t40. 30.
+INTEGRATOR\tBM4
+DT\t\t.1
+TINTEGRATION\t50
+DT_SAVE\t\t1.
+N_OBSERVABLES\t6
+OBSERVABLES\tdipole_r dipole_v energy PED PMD wavefunction
+P_MAX\t\t3.
+R_MASK\t\t5. 10.
+DE\t\t.05
+NE\t\t40
+"""
+
+
+def test_real_driver_rejects_bad_parameter_files(driver, tmp_path):
+    from tdse_nd_mpi_b200.build import build_drivers
+
+    build_drivers()
+    (tmp_path / "output.imag").write_bytes(b"DIMENSION\t1\nN_STATES\t2\nNR\t256\nDR\t0.2\nPOTENTIAL\tH_1D\n"
+                                            b"E\t\t-0.5\t-0.1\nDE\t0\t0\nPSI\n" + bytes(16 * 512))
+    p = tmp_path / "params.real"
+    p.write_text(PARAMS_REAL.format(gauge="length") + "FOO 1\n")
+    r = subprocess.run([REAL_DRIVER, str(p)], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 1 and "Unknown parameter: FOO" in r.stdout
+    p.write_text(PARAMS_REAL.format(gauge="length"))
+    r = subprocess.run([REAL_DRIVER, str(p), "NR", "256"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 1 and "Unrecognized parameter key 'NR'" in r.stderr
+
+
+def _text_table(path):
+    rows = [line.split() for line in open(path).read().splitlines() if line.strip()]
+    return rows[0], np.array(rows[1:], dtype=float)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("gauge", ["length", "velocity"])
+def test_real_driver_outputs_match_reference_executable(driver, tmp_path, gauge):
+    """QuantumND_real end to end (two-state superposition read from output.imag onto a larger grid,
+    two laser modes, CAP, observables every step, PED/PMD/wavefunction) against the reference's
+    executable on the same inputs: every output file."""
+    from oracle import oracle as O
+
+    if not (os.path.exists(REF_IMAG) and os.path.exists(REF_REAL)):
+        pytest.skip("reference executables not built")
+    seed = tmp_path / "seed"
+    seed.mkdir()
+    assert run(REF_IMAG, PARAMS.replace("TINTEGRATION \t30", "TINTEGRATION \t20"), seed).returncode == 0
+    out = {}
+    for who, exe in (("ours", REAL_DRIVER), ("ref", REF_REAL)):
+        d = tmp_path / who
+        d.mkdir()
+        (d / "output.imag").write_bytes((seed / "output.imag").read_bytes())
+        (d / "params.real").write_text(PARAMS_REAL.format(gauge=gauge))
+        r = subprocess.run([exe, "params.real"], cwd=d, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, (who, r.stdout[-2000:], r.stderr[-2000:])
+        out[who] = d
+    h1, o1 = _text_table(out["ours"] / "observables.real")
+    h2, o2 = _text_table(out["ref"] / "observables.real")
+    assert h1 == h2 and o1.shape == o2.shape
+    np.testing.assert_allclose(o1, o2, rtol=1e-9, atol=1e-12)
+    for f in ("electric_field.real", "vector_potential.real"):
+        a = np.loadtxt(out["ours"] / f)
+        b = np.loadtxt(out["ref"] / f)
+        np.testing.assert_allclose(a, b, rtol=1e-13, atol=1e-15)
+    ped1, ped2 = np.loadtxt(out["ours"] / "PED.real"), np.loadtxt(out["ref"] / "PED.real")
+    np.testing.assert_allclose(ped1, ped2, rtol=0, atol=1e-10 * np.abs(ped2[:, 1]).max())
+    (hd1, d1), (hd2, d2) = O.read_pmd(out["ours"] / "PMD.real"), O.read_pmd(out["ref"] / "PMD.real")
+    assert hd1 == hd2 and d1.shape == d2.shape
+    np.testing.assert_allclose(d1[:, 0], d2[:, 0], rtol=0, atol=1e-10 * d2[:, 0].max())
+    w1 = open(out["ours"] / "wavefunction.real", "rb").read()
+    w2 = open(out["ref"] / "wavefunction.real", "rb").read()
+    k1, k2 = w1.index(b"PSI_BINARY_START\n") + 17, w2.index(b"PSI_BINARY_START\n") + 17
+    assert w1[:k1] == w2[:k2]
+    p1, p2 = np.frombuffer(w1[k1:], np.complex128), np.frombuffer(w2[k2:], np.complex128)
+    assert np.linalg.norm(p1 - p2) / np.linalg.norm(p2) < 1e-9
