@@ -195,6 +195,21 @@ def cpu_reference_steps(max_steps, budget_s):
     return {"value": 1.0 / per_step, "unit": "steps/s", "cores": nthreads, "kind": kind, "sample": sample}
 
 
+def max_over_ranks(torch, dist, value, device):
+    """The largest of a per-rank float over all ranks (the slowest rank sets the job's time); the
+    value itself when there is no process group."""
+    if dist is None:
+        return float(value)
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, steps, ms):
+    """Whole-job steps/s: every rank (replica) runs `steps` steps, the job takes `ms`."""
+    return world * steps / (ms / 1000.0)
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -425,11 +440,8 @@ def main():
     with ClockSampler(local) as clk:
         total_ms = timed_steps(torch, grid, psi_t, E_dev, obs_dev, OBS, i0, args.steps, args.warmup, flush)
     grid.get_profile(reset=True)
-    if dist:
-        tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
-    value = world * args.steps / (total_ms / 1000.0)
+    total_ms = max_over_ranks(torch, dist, total_ms, dev)
+    value = job_throughput(world, args.steps, total_ms)
     ms_step = total_ms / args.steps
     obs_fp64 = obs_dev[args.warmup:].cpu().numpy()
 
@@ -500,12 +512,8 @@ def main():
     h3 = time.perf_counter()
     b.record()
     torch.cuda.synchronize()
-    e2e_ms = a.elapsed_time(b)
-    if dist:
-        tt = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
-    e2e = {"value": world * e2e_steps / (e2e_ms / 1000.0), "unit": "steps/s",
+    e2e_ms = max_over_ranks(torch, dist, a.elapsed_time(b), dev)
+    e2e = {"value": job_throughput(world, e2e_steps, e2e_ms), "unit": "steps/s",
            "h2d_bytes_per_step": (n * 16 + e2e_steps * grid.s * 2 * 8) / e2e_steps,
            "d2h_bytes_per_step": (n * 16 + e2e_steps * nv * 8) / e2e_steps,
            "what": "qnd_state_upload + qnd_run_length (host E, host observable rows) + qnd_state_download",
@@ -517,7 +525,8 @@ def main():
         gm = setup_grid(torch, "mixed", V, grads, mask, stream)
         psi_m = torch.tensor(psi0.astype(np.complex64).view(np.float32), device=dev).contiguous()
         obs_m = torch.zeros_like(obs_dev)
-        ms_m = timed_steps(torch, gm, psi_m, E_dev, obs_m, OBS, i0, args.steps, args.warmup, flush) / args.steps
+        ms_m = max_over_ranks(torch, dist, timed_steps(torch, gm, psi_m, E_dev, obs_m, OBS, i0, args.steps,
+                                                      args.warmup, flush), dev) / args.steps
         om = obs_m[args.warmup:].cpu().numpy()
         # error of each observable relative to its own magnitude over the run; observables that vanish
         # by symmetry (y-dipole, y-acceleration under x polarisation) are reported as absolute errors
