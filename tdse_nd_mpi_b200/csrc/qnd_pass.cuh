@@ -175,58 +175,58 @@ __device__ __forceinline__ void accumulate_red(const RedDesc& rd, double* acc, V
     }
 }
 
-// Reductions over the E values a thread holds of one line (m = tid + u*T), in chunks of C values
-// (accumulator-inner within a chunk) so that few FP64 temporaries are live at once; weights along
-// the pass axis are read per element, weights along other axes once per chunk, full-grid weights
-// from the line-major table.
+// Reductions over the E values a thread holds of one line (m = tid + u*T), accumulator-outer: for
+// each accumulator the weights are either a per-line scalar (weight 1, or a weight along another
+// axis) or a row read with stride T (a weight along the pass axis, or the line's row of a line-major
+// full-grid table), so one loop serves both; |v|^2 is recomputed per accumulator (two FMAs) rather
+// than held in E extra FP64 registers.
 template <typename R, int E, int T>
 __device__ __forceinline__ void accumulate_line(const RedDesc& rd, double* acc, const cplx_t<R>* v,
                                                 const cplx_t<R>* partner, long long base, int log2S, long long lbase,
                                                 int tid, int axis, const int* shift, const long long* nmask) {
-    constexpr int C = E < 4 ? E : 4;
 #pragma unroll
-    for (int u0 = 0; u0 < E; u0 += C) {
-        double a2[C];
+    for (int k = 0; k < MAX_RED; ++k) {
+        if (k >= rd.n) break;
+        double sum = 0.0;
+        const int wk = rd.wkind[k];
+        const double* __restrict__ wt = rd.wtab[k];
+        if (rd.kind[k] == RK_ABS2) {
+            const double* __restrict__ row = nullptr;  // stride-T weights of this line
+            double wl = 1.0;                           // or one weight for the whole line
+            if (wk == WK_GRID) {
+                row = wt + lbase + tid;
+            } else if (wk == WK_AXIS) {
+                const int ax = rd.waxis[k];
+                if (ax == axis) row = wt + tid;
+                else wl = __ldg(wt + ((base >> shift[ax]) & nmask[ax]));
+            }
+            if (row) {
 #pragma unroll
-        for (int c = 0; c < C; ++c)
-            a2[c] = double(v[u0 + c].x) * double(v[u0 + c].x) + double(v[u0 + c].y) * double(v[u0 + c].y);
-#pragma unroll
-        for (int k = 0; k < MAX_RED; ++k) {
-            if (k >= rd.n) break;
-            double sum = 0.0;
-            const int wk = rd.wkind[k];
-            const double* __restrict__ wt = rd.wtab[k];
-            if (rd.kind[k] == RK_ABS2) {
-                if (wk == WK_ONE) {
-#pragma unroll
-                    for (int c = 0; c < C; ++c) sum += a2[c];
-                } else if (wk == WK_AXIS && rd.waxis[k] == axis) {
-#pragma unroll
-                    for (int c = 0; c < C; ++c) sum += a2[c] * __ldg(wt + tid + (u0 + c) * T);
-                } else if (wk == WK_AXIS) {
-                    const int ax = rd.waxis[k];
-                    const double wl = __ldg(wt + ((base >> shift[ax]) & nmask[ax]));
-#pragma unroll
-                    for (int c = 0; c < C; ++c) sum += a2[c];
-                    sum *= wl;
-                } else {
-#pragma unroll
-                    for (int c = 0; c < C; ++c) sum += a2[c] * __ldg(wt + lbase + tid + (u0 + c) * T);
+                for (int u = 0; u < E; ++u) {
+                    const double x = v[u].x, y = v[u].y;
+                    sum = fma(fma(x, x, y * y), __ldg(row + u * T), sum);
                 }
             } else {
 #pragma unroll
-                for (int c = 0; c < C; ++c) {
-                    const int m = tid + (u0 + c) * T;
-                    const long long flat = base + ((long long)m << log2S);
-                    const cplx_t<R> p = partner[flat];
-                    double val = double(p.x) * double(v[u0 + c].x) + double(p.y) * double(v[u0 + c].y);
-                    if (wk == WK_AXIS) val *= __ldg(wt + ((flat >> shift[rd.waxis[k]]) & nmask[rd.waxis[k]]));
-                    else if (wk == WK_GRID) val *= __ldg(wt + lbase + m);
-                    sum += val;
+                for (int u = 0; u < E; ++u) {
+                    const double x = v[u].x, y = v[u].y;
+                    sum += fma(x, x, y * y);
                 }
+                sum *= wl;
             }
-            acc[k] += sum;
+        } else {
+#pragma unroll
+            for (int u = 0; u < E; ++u) {
+                const int m = tid + u * T;
+                const long long flat = base + ((long long)m << log2S);
+                const cplx_t<R> p = partner[flat];
+                double val = double(p.x) * double(v[u].x) + double(p.y) * double(v[u].y);
+                if (wk == WK_AXIS) val *= __ldg(wt + ((flat >> shift[rd.waxis[k]]) & nmask[rd.waxis[k]]));
+                else if (wk == WK_GRID) val *= __ldg(wt + lbase + m);
+                sum += val;
+            }
         }
+        acc[k] += sum;
     }
 }
 
