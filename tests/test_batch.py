@@ -1,0 +1,91 @@
+"""Sweeps of independent members (tdse_nd_mpi_b200/batch.py): the balanced partition and the
+rank-0 gather on two gloo ranks on the CPU; on the GPU, concurrent members against one-by-one runs."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from tdse_nd_mpi_b200.batch import Member, partition, run_sharded
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _member(shape, seed, integ="BM4", nsteps=4):
+    rng = np.random.default_rng(seed)
+    dim = len(shape)
+    s = {"BM4": 6, "Verlet": 1}[integ]
+    psi = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    return Member(shape=shape, dr=(0.3,) * dim, integrator=integ, dt=0.05, potential="H_2D" if dim == 2 else "H_1D",
+                  field=rng.standard_normal((nsteps, s, dim)) * 0.05, psi0=psi / np.linalg.norm(psi), cap=(0.1, 2.0))
+
+
+def test_partition_balances_bytes_and_covers_every_member():
+    # the sweep configuration's mix: 32 x 256^2, 48 x 512^2, 16 x 1024^2
+    members = [_member((256, 256), 0)] * 32 + [_member((512, 512), 0)] * 48 + [_member((1024, 1024), 0)] * 16
+    for world in (1, 2, 4, 8):
+        parts = partition(members, world)
+        assert sorted(i for p in parts for i in p) == list(range(len(members)))
+        loads = [sum(members[i].state_bytes for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(m.state_bytes for m in members)
+        assert parts == partition(members, world)          # the same on every rank
+
+
+def _fake_runner(ms):
+    return [{"obs": np.full((1, 1), float(np.prod(m.shape))), "psi": None} for m in ms]
+
+
+def _rank(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        members = [_member((n, n), i) for i, n in enumerate((8, 16, 32, 16, 8))]
+        out = run_sharded(members, dist, runner=_fake_runner)
+        q.put((rank, None if out is None else [float(r["obs"][0, 0]) for r in out]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_gather_every_member_in_order():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert got[1] is None
+    assert got[0] == [64.0, 256.0, 1024.0, 256.0, 64.0]
+
+
+@pytest.mark.gpu
+def test_concurrent_members_match_one_by_one(qnd_lib):
+    from tdse_nd_mpi_b200 import Grid
+    from tdse_nd_mpi_b200.batch import run_members
+    import torch
+
+    members = [_member((128, 128), 1), _member((256, 256), 2, "Verlet"), _member((64, 128), 3), _member((1024,), 4)]
+    together = run_members(members)
+    for m, r in zip(members, together):
+        g = Grid(len(m.shape), m.shape, m.dr, m.integrator, m.dt)
+        g.set_potential(m.potential)
+        g.set_cap(*m.cap)
+        st = g.state(m.psi0)
+        E = torch.tensor(m.field, device="cuda")
+        obs = torch.zeros((E.shape[0], g.nvalues(list(m.names))), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        g.run_length_dev(st, E, E.shape[0], list(m.names), obs)
+        g.synchronize()
+        np.testing.assert_array_equal(obs.cpu().numpy(), r["obs"])
+        np.testing.assert_array_equal(st.download(), r["psi"])
+        g.close()
