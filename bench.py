@@ -461,7 +461,7 @@ def main():
     flush_every_step = {"value": 1000.0 / ms_fs, "unit": "steps/s", "ms_per_step": ms_fs, "steps": fs_steps,
                         "what": "rank-local: one qnd_run_length_dev call per step, 256 MB L2 flush before each step"}
     n = NR * NR
-    # Algorithmic bytes (the survey's accounting): every full-grid N-D transform is one read and one
+    # Algorithmic bytes (the metric's accounting): every full-grid N-D transform is one read and one
     # write of the state, 2*N*16 bytes; a BM4 length-gauge step is 2s = 12 transforms plus the 2 of
     # the per-step observable round trip, 14 in all. The engine does that work in fewer, fused passes
     # (two-sandwich passes), so the per-launch figure is the step's algorithmic bytes over its launches.
