@@ -261,6 +261,74 @@ template <typename R> void launch_pmd(const SpectraArgs& a, const cplx_t<R>* psi
     pmd_kernel<R><<<(int)nb, 256, 0, st>>>(a, psi_p, out);
 }
 
+// ---- axes longer than one pass: the four-step pieces (qnd_engine.cu, long_fft) -------
+
+template <typename R>
+__global__ void __launch_bounds__(256) long_twiddle_kernel(long long n, cplx_t<R>* psi, const cplx_t<R>* w, int conj) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        cplx_t<R> f = w[i];
+        if (conj) f.y = -f.y;  // conj(w) and, for FP32 tables, conj(w - 1) = conj(w) - 1
+        psi[i] = fmul(psi[i], f);
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) long_transpose_kernel(LongArgs a, const cplx_t<R>* in, cplx_t<R>* out,
+                                                             int to_natural) {
+    const long long m2 = (1ll << a.log2n2) - 1;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (long long)gridDim.x * blockDim.x) {
+        const long long k = (i >> a.log2n2) + ((i & m2) << a.log2n1);  // slot i holds natural index k
+        if (to_natural) out[k] = in[i];
+        else out[i] = in[k];
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) point_factors_kernel(long long n, cplx_t<R>* psi, const R* tr,
+                                                            const cplx_t<R>* tc, const cplx_t<R>* pc, const R* pr,
+                                                            const double* scale_dev) {
+    const R sc = scale_dev ? R(*scale_dev) : R(1);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        cplx_t<R> x = psi[i];
+        if (tr) x = cscale(x, tr[i]);
+        if (tc) x = fmul(x, tc[i]);
+        if (pc) x = fmul(x, pc[i]);
+        if (pr) x = cscale(x, pr[i]);
+        if (scale_dev) x = cscale(x, sc);
+        psi[i] = x;
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) add_potential_kernel(long long n, cplx_t<R>* dst, const cplx_t<R>* src,
+                                                            const double* vtab) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = cadd(dst[i], cscale(src[i], R(vtab[i])));
+}
+
+static int elementwise_blocks(long long n) {
+    long long nb = (n + 255) / 256;
+    if (nb > 148 * 16) nb = 148 * 16;
+    return int(nb < 1 ? 1 : nb);
+}
+template <typename R> void launch_long_twiddle(const LongArgs& a, cplx_t<R>* psi, const cplx_t<R>* w, int conj,
+                                               cudaStream_t st) {
+    long_twiddle_kernel<R><<<elementwise_blocks(a.n), 256, 0, st>>>(a.n, psi, w, conj);
+}
+template <typename R> void launch_long_transpose(const LongArgs& a, const cplx_t<R>* in, cplx_t<R>* out, int to_natural,
+                                                 cudaStream_t st) {
+    long_transpose_kernel<R><<<elementwise_blocks(a.n), 256, 0, st>>>(a, in, out, to_natural);
+}
+template <typename R> void launch_point_factors(long long n, cplx_t<R>* psi, const R* tr, const cplx_t<R>* tc,
+                                                const cplx_t<R>* pc, const R* pr, const double* scale_dev,
+                                                cudaStream_t st) {
+    point_factors_kernel<R><<<elementwise_blocks(n), 256, 0, st>>>(n, psi, tr, tc, pc, pr, scale_dev);
+}
+template <typename R> void launch_add_potential(long long n, cplx_t<R>* dst, const cplx_t<R>* src, const double* vtab,
+                                                cudaStream_t st) {
+    add_potential_kernel<R><<<elementwise_blocks(n), 256, 0, st>>>(n, dst, src, vtab);
+}
+
 #define QND_INST(R)                                                                               \
     template void launch_gs_dot<R>(const GSArgs<R>&, cudaStream_t, int);                          \
     template void launch_gs_axpy<R>(const GSArgs<R>&, cudaStream_t, int);                         \
@@ -270,7 +338,12 @@ template <typename R> void launch_pmd(const SpectraArgs& a, const cplx_t<R>* psi
     template void launch_axis_table<R>(int, const double*, int, double, void*, cudaStream_t);             \
     template void launch_radial_mask<R>(const SpectraArgs&, const cplx_t<R>*, cplx_t<R>*, cudaStream_t);  \
     template void launch_ped<R>(const SpectraArgs&, const cplx_t<R>*, double*, double*, cudaStream_t);    \
-    template void launch_pmd<R>(const SpectraArgs&, const cplx_t<R>*, double*, cudaStream_t);
+    template void launch_pmd<R>(const SpectraArgs&, const cplx_t<R>*, double*, cudaStream_t);             \
+    template void launch_long_twiddle<R>(const LongArgs&, cplx_t<R>*, const cplx_t<R>*, int, cudaStream_t); \
+    template void launch_long_transpose<R>(const LongArgs&, const cplx_t<R>*, cplx_t<R>*, int, cudaStream_t); \
+    template void launch_point_factors<R>(long long, cplx_t<R>*, const R*, const cplx_t<R>*, const cplx_t<R>*, \
+                                          const R*, const double*, cudaStream_t);                          \
+    template void launch_add_potential<R>(long long, cplx_t<R>*, const cplx_t<R>*, const double*, cudaStream_t);
 QND_INST(double)
 QND_INST(float)
 #undef QND_INST

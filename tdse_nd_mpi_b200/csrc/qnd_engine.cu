@@ -105,6 +105,7 @@ struct ObsItem {
 };
 
 static const double MAX_EXP_ARG = 700.;  // integrators.h:12
+static const int64_t LONG_AXIS_MAX = int64_t(1) << 24;  // longest 1-D axis (four-step transform)
 
 }  // namespace qnd
 
@@ -149,6 +150,17 @@ struct qnd_ctx {
     DevBuf field_dev, field_tab, wtab_dev[MAX_DIM], spec_tmp[MAX_DIM];
     DevBuf scratch_a, scratch_b;
     DevBuf spec_rank, spec_partials, spec_out;  // final spectra: per-axis ranks, partial sums, results
+
+    // A 1-D axis longer than one pass handles: N = n1 n2 (n1 >= 16, n2 <= 4096) as a virtual
+    // n1 x n2 grid transformed in four steps (long_fft). tw_long[v]: the stage twiddles of the
+    // length-n1 (v = 0) and length-n2 (v = 1) passes; twf_long / twc_long: the four-step twiddle
+    // W_N^{k1 m} and its conjugate at slot k1 n2 + m; p_slot: the momentum of each k-space slot
+    // (slot k1 n2 + k2 holds frequency k1 + n1 k2).
+    bool long1d = false;
+    int64_t n1 = 0, n2 = 0;
+    int lg1 = 0, lg2 = 0;
+    DevBuf tw_long[2], twf_long, twc_long, p_slot_dev, long_tmp;
+    std::vector<double> p_slot;
     std::vector<char> host_tmp;
 
     int num_sms = 148;
@@ -221,8 +233,7 @@ static void round_pairs_f32_balanced(const double* v, size_t n, float* out) {
 }
 
 // Twiddles of HostPlan(L) in the [j mod Ns][r-1] layout, exp(-2 pi i jm r / (Ns R)), in long double.
-static void build_twiddles(qnd_ctx* c, int ax) {
-    const int L = int(c->nr[ax]);
+static void build_twiddles(qnd_ctx* c, int L, DevBuf& dst) {
     HostPlan pl(L, lookup_pass(c->fp64, L, false, PM_SANDWICH).E);
     std::vector<double> tw(2 * size_t(pl.tw_size > 0 ? pl.tw_size : 1));
     const long double two_pi = 6.283185307179586476925286766559005768L;
@@ -243,13 +254,13 @@ static void build_twiddles(qnd_ctx* c, int ax) {
             }
     }
     const size_t cnt = size_t(pl.tw_size > 0 ? pl.tw_size : 1);
-    c->tw[ax].ensure(cnt * c->elem());
+    dst.ensure(cnt * c->elem());
     if (c->fp64) {
-        QND_CK(cudaMemcpyAsync(c->tw[ax].p, tw.data(), cnt * 16, cudaMemcpyHostToDevice, c->stream));
+        QND_CK(cudaMemcpyAsync(dst.p, tw.data(), cnt * 16, cudaMemcpyHostToDevice, c->stream));
     } else {
         std::vector<float> f(2 * cnt);
         round_pairs_f32_balanced(tw.data(), cnt, f.data());
-        QND_CK(cudaMemcpyAsync(c->tw[ax].p, f.data(), cnt * 8, cudaMemcpyHostToDevice, c->stream));
+        QND_CK(cudaMemcpyAsync(dst.p, f.data(), cnt * 8, cudaMemcpyHostToDevice, c->stream));
     }
 }
 
@@ -304,25 +315,28 @@ static const void* spec_table(qnd_ctx* c, int kind, int ax, double coef) {
     auto it = c->spec_cache.find(key);
     if (it != c->spec_cache.end()) return it->second->p;
     const int N = int(c->nr[ax]);
+    // a long axis: slot order, and the 1/N of the inverse transform split as 1/n2 here (FP64; FP32
+    // tables are scaled by 1/n2 in the pass) and 1/n1 in the closing length-n1 pass
+    const double Nn = c->long1d ? double(c->n2) : double(N);
     std::vector<double> v(2 * size_t(N));
     for (int k = 0; k < N; ++k) {
-        const double pk = c->p[ax][k];
+        const double pk = c->long1d ? c->p_slot[k] : c->p[ax][k];
         const double kin = .5 * pk * pk;
         double re, im;
         if (kind == SP_LENGTH) {
             const double th = coef * kin;
             if (c->fp64) {
-                re = std::cos(th) / N;
+                re = std::cos(th) / Nn;
             } else {
                 const double sh = std::sin(th / 2);
                 re = -2 * sh * sh;
             }
-            im = c->fp64 ? -std::sin(th) / N : -std::sin(th);
+            im = c->fp64 ? -std::sin(th) / Nn : -std::sin(th);
         } else if (kind == SP_IMAG) {
-            re = c->fp64 ? std::exp(-coef * kin) / N : std::expm1(-coef * kin);
+            re = c->fp64 ? std::exp(-coef * kin) / Nn : std::expm1(-coef * kin);
             im = 0;
         } else {
-            re = c->fp64 ? kin / N : kin - 1.0;
+            re = c->fp64 ? kin / Nn : kin - 1.0;
             im = 0;
         }
         v[2 * k] = re;
@@ -469,6 +483,10 @@ struct PassSpec {
     int apply_acc = 0;
     const double* apply_vtab = nullptr;
     RedDesc red{};
+    int spec_full = 0;           // spec: a full-grid table in line-major order
+    // a pass over a virtual axis of a long 1-D axis: its length, log2 stride and stage twiddles
+    int vL = 0, vlog2S = 0;
+    const void* vtw = nullptr;
 };
 
 static void ensure_red_scratch(qnd_ctx* c, long long blocks) {
@@ -496,6 +514,7 @@ template <typename R> static void fill_args(qnd_ctx* c, const PassSpec& ps, Pass
     a.pro_cplx = static_cast<const V*>(ps.pro_cplx);
     a.pro_scale_dev = ps.pro_scale;
     a.spec = static_cast<const V*>(ps.spec);
+    a.spec_full = ps.spec_full;
     a.spec2 = static_cast<const V*>(ps.spec2);
     a.mid_real = static_cast<const R*>(ps.mid_real);
     a.mid_cplx = static_cast<const V*>(ps.mid_cplx);
@@ -526,8 +545,9 @@ struct LaunchCfg {
 // dependent launch so the pass's prologue overlaps the tail of the previous kernel.
 static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     const int ax = ps.axis;
-    const int L = int(c->nr[ax]);
-    const int log2S = c->shift[ax];
+    const int L = ps.vL ? ps.vL : int(c->nr[ax]);
+    const int log2S = ps.vL ? ps.vlog2S : c->shift[ax];
+    const void* tw = ps.vL ? ps.vtw : c->tw[ax].p;
     const bool strided = log2S > 0;
     const PassKernelInfo info = lookup_pass(c->fp64, L, strided, ps.mode);
     const long long nlines = c->n / L;
@@ -575,7 +595,7 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         PassArgs<double> a;
         fill_args<double>(c, ps, a);
         a.red = red;
-        a.tw = c->tw[ax].as<double2>();
+        a.tw = static_cast<const double2*>(tw);
         a.log2S = log2S;
         a.nlines = nlines;
         void* args[] = {&a};
@@ -584,7 +604,7 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         PassArgs<float> a;
         fill_args<float>(c, ps, a);
         a.red = red;
-        a.tw = c->tw[ax].as<float2>();
+        a.tw = static_cast<const float2*>(tw);
         a.log2S = log2S;
         a.nlines = nlines;
         void* args[] = {&a};
@@ -604,7 +624,7 @@ static int reduce_blocks(qnd_ctx* c) {
 }
 
 // Element-wise r-space reductions of psi.
-static void grid_reduce(qnd_ctx* c, const void* psi, const RedDesc& rd_in) {
+static void grid_reduce(qnd_ctx* c, const void* psi, const RedDesc& rd_in, const void* partner = nullptr) {
     RedDesc rd = rd_in;
     const int nb = reduce_blocks(c);
     ensure_red_scratch(c, nb);
@@ -612,6 +632,7 @@ static void grid_reduce(qnd_ctx* c, const void* psi, const RedDesc& rd_in) {
     rd.counter = c->counter.as<unsigned int>();
     PassSpec ps;
     ps.psi = const_cast<void*>(psi);
+    ps.partner = partner;
     ps.red = rd;
     if (c->fp64) {
         PassArgs<double> a;
@@ -631,6 +652,114 @@ static std::vector<int> pass_order(const qnd_ctx* c) {
     std::vector<int> o;
     for (int k = c->dim - 1; k >= 0; --k) o.push_back(k);
     return o;
+}
+
+// ---------------------------------------------------------------- long axes --
+//
+// A 1-D axis of N = n1 n2 points (n2 = min(4096, N / 16), n1 = N / n2) is transformed in four
+// steps over the virtual n1 x n2 grid in which point n1_ n2 + n2_ sits (natural order):
+//   F[k1 + n1 k2] = sum_{n2_} W_{n2}^{n2_ k2} W_N^{n2_ k1} sum_{n1_} W_{n1}^{n1_ k1} psi[n1_ n2 + n2_]
+// i.e. length-n1 transforms along the strided virtual axis, the twiddles W_N^{k1 n2_}, then
+// length-n2 transforms along the contiguous one; the spectrum lands in slot order (slot k1 n2 + k2
+// holds frequency k1 + n1 k2), where every k-space table of the axis is stored. A kinetic sandwich
+// F^-1 K F is three passes: length-n1 forward; one length-n2 sandwich pass with the twiddles as its
+// prologue, the slot-order table K as its spectral factor and the conjugate twiddles as its
+// epilogue; length-n1 inverse carrying the last 1/n1. The r-space work between sandwiches (factor
+// tables, laser phases, the mask, reductions) runs as element-wise kernels in natural order.
+
+static PassSpec long_pass(qnd_ctx* c, int v, int mode, void* psi, double scale) {
+    PassSpec ps;
+    ps.axis = 0;
+    ps.mode = mode;
+    ps.psi = psi;
+    ps.scale = scale;
+    ps.vL = int(v == 0 ? c->n1 : c->n2);
+    ps.vlog2S = v == 0 ? c->lg2 : 0;
+    ps.vtw = c->tw_long[v].p;
+    return ps;
+}
+
+static LongArgs long_args(const qnd_ctx* c) {
+    LongArgs a{};
+    a.n = c->n;
+    a.log2n1 = c->lg1;
+    a.log2n2 = c->lg2;
+    return a;
+}
+
+static void long_twiddle(qnd_ctx* c, void* psi, bool conj) {
+    if (c->fp64)
+        launch_long_twiddle<double>(long_args(c), static_cast<double2*>(psi), c->twf_long.as<double2>(), conj, c->stream);
+    else
+        launch_long_twiddle<float>(long_args(c), static_cast<float2*>(psi), c->twf_long.as<float2>(), conj, c->stream);
+    c->kernels_launched++;
+    QND_CK(cudaGetLastError());
+}
+
+// Unnormalised transform (times s1 s2): forward from natural order into slot order, inverse back.
+static void long_fft(qnd_ctx* c, void* psi, bool forward, double s1, double s2) {
+    if (forward) {
+        launch_pass(c, long_pass(c, 0, PM_FFT_FWD, psi, s1));
+        long_twiddle(c, psi, false);
+        launch_pass(c, long_pass(c, 1, PM_FFT_FWD, psi, s2));
+    } else {
+        launch_pass(c, long_pass(c, 1, PM_FFT_INV, psi, s2));
+        long_twiddle(c, psi, true);
+        launch_pass(c, long_pass(c, 0, PM_FFT_INV, psi, s1));
+    }
+}
+
+// psi <- F^-1 spec F psi for a slot-order spectral table (1/N included as described above).
+static void long_sandwich(qnd_ctx* c, void* psi, const void* spec) {
+    launch_pass(c, long_pass(c, 0, PM_FFT_FWD, psi, 1.0));
+    PassSpec ps = long_pass(c, 1, PM_SANDWICH, psi, 1.0);
+    ps.pro_cplx = c->twf_long.p;
+    ps.spec = spec;
+    ps.spec_full = 1;
+    ps.epi_cplx = c->twc_long.p;
+    launch_pass(c, ps);
+    launch_pass(c, long_pass(c, 0, PM_FFT_INV, psi, 1.0 / double(c->n1)));
+}
+
+// Slot order <-> natural order, through the context's long-axis scratch state.
+static void long_reorder(qnd_ctx* c, void* psi, bool to_natural) {
+    c->long_tmp.ensure(size_t(c->n) * c->elem());
+    if (c->fp64)
+        launch_long_transpose<double>(long_args(c), static_cast<const double2*>(psi), c->long_tmp.as<double2>(),
+                                      to_natural, c->stream);
+    else
+        launch_long_transpose<float>(long_args(c), static_cast<const float2*>(psi), c->long_tmp.as<float2>(),
+                                     to_natural, c->stream);
+    c->kernels_launched++;
+    QND_CK(cudaGetLastError());
+    QND_CK(cudaMemcpyAsync(psi, c->long_tmp.p, size_t(c->n) * c->elem(), cudaMemcpyDeviceToDevice, c->stream));
+}
+
+static void long_point(qnd_ctx* c, void* psi, const void* treal, const void* tcplx, const void* pcplx, const void* preal,
+                       const double* scale_dev) {
+    if (!treal && !tcplx && !pcplx && !preal && !scale_dev) return;
+    if (c->fp64)
+        launch_point_factors<double>(c->n, static_cast<double2*>(psi), static_cast<const double*>(treal),
+                                     static_cast<const double2*>(tcplx), static_cast<const double2*>(pcplx),
+                                     static_cast<const double*>(preal), scale_dev, c->stream);
+    else
+        launch_point_factors<float>(c->n, static_cast<float2*>(psi), static_cast<const float*>(treal),
+                                    static_cast<const float2*>(tcplx), static_cast<const float2*>(pcplx),
+                                    static_cast<const float*>(preal), scale_dev, c->stream);
+    c->kernels_launched++;
+    QND_CK(cudaGetLastError());
+}
+
+// dst = H src = F^-1 (p^2/2) F src + V src (the kinetic operator of calculate_observables.c:165).
+static void long_apply_h(qnd_ctx* c, const void* src, void* dst, const void* kin_spec, const double* vpot) {
+    QND_CK(cudaMemcpyAsync(dst, src, size_t(c->n) * c->elem(), cudaMemcpyDeviceToDevice, c->stream));
+    long_sandwich(c, dst, kin_spec);
+    if (c->fp64)
+        launch_add_potential<double>(c->n, static_cast<double2*>(dst), static_cast<const double2*>(src), vpot, c->stream);
+    else
+        launch_add_potential<float>(c->n, static_cast<float2*>(dst), static_cast<const float2*>(src), vpot, c->stream);
+    c->kernels_launched++;
+    QND_CK(cudaGetLastError());
 }
 
 // ---------------------------------------------------------------- observables --
@@ -723,6 +852,18 @@ static void energy_moments(qnd_ctx* c, const void* psi, int nmom, double* out_de
     auto order = pass_order(c);
     for (int m = 1; m <= nmom; ++m) {
         void* dst = (m % 2) ? c->scratch_a.p : c->scratch_b.p;
+        if (c->long1d) {
+            long_apply_h(c, src, dst, spec_table(c, SP_KIN, 0, 0.0), c->vpot_dev.as<double>());
+            RedDesc rd{};
+            rd.n = 1;
+            rd.kind[0] = RK_BILIN;
+            rd.wkind[0] = WK_ONE;
+            rd.scale[0] = c->dNr;
+            rd.out = out_dev + (m - 1);
+            grid_reduce(c, dst, rd, psi);
+            src = dst;
+            continue;
+        }
         for (size_t q = 0; q < order.size(); ++q) {
             const int ax = order[q];
             PassSpec ps;
@@ -754,6 +895,27 @@ static void eval_obs(qnd_ctx* c, const void* psi, const std::vector<ObsItem>& it
     for (auto& it : items) {
         if (it.kind == OB_DIPOLE_V) {
             // sum_k |psi~|^2 (p_j + alpha_j) dNp fft_scaling = (dNp/N_j) sum |F_j psi|^2 (p_j + alpha_j)
+            if (c->long1d) {
+                // |F psi|^2 in slot order, weighted by the slot momenta
+                c->long_tmp.ensure(size_t(c->n) * c->elem());
+                QND_CK(cudaMemcpyAsync(c->long_tmp.p, psi, size_t(c->n) * c->elem(), cudaMemcpyDeviceToDevice,
+                                       c->stream));
+                long_fft(c, c->long_tmp.p, true, 1.0, 1.0);
+                c->wtab_dev[0].ensure(size_t(c->n) * 8);
+                launch_axis_table<double>(0, c->p_slot_dev.as<double>(), int(c->n), alpha[0], c->wtab_dev[0].p,
+                                          c->stream);
+                c->kernels_launched++;
+                RedDesc rd{};
+                rd.n = 1;
+                rd.kind[0] = RK_ABS2;
+                rd.wkind[0] = WK_AXIS;
+                rd.waxis[0] = 0;
+                rd.wtab[0] = c->wtab_dev[0].as<double>();
+                rd.scale[0] = c->dNp / double(c->n);
+                rd.out = row_dev + it.offset;
+                grid_reduce(c, c->long_tmp.p, rd);
+                continue;
+            }
             for (int j = 0; j < c->dim; ++j) {
                 c->wtab_dev[j].ensure(size_t(c->nr[j]) * 8);
                 if (c->fp64)
@@ -839,12 +1001,13 @@ static void check_imag_clamp(qnd_ctx* c) {
 static void build_field_tables(qnd_ctx* c, const double* field_dev, int64_t nsteps, bool velocity) {
     FieldTableArgs fa{};
     fa.field = field_dev;
-    fa.axes = velocity ? c->p_dev.as<double>() : c->r_dev.as<double>();
+    // velocity tables of a long axis: slot order (k-space tables), the 1/n2 of its sandwich pass
+    fa.axes = velocity ? (c->long1d ? c->p_slot_dev.as<double>() : c->p_dev.as<double>()) : c->r_dev.as<double>();
     fa.nsteps = int(nsteps);
     fa.s = c->s;
     fa.dim = c->dim;
     for (int j = 0; j < c->dim; ++j) {
-        fa.nr[j] = int(c->nr[j]);
+        fa.nr[j] = int(c->long1d ? c->n2 : c->nr[j]);
         fa.off[j] = c->axoff[j];
     }
     fa.ntot = c->axtot;
@@ -940,6 +1103,23 @@ static void run_chain(qnd_ctx* c, void* psi, const std::vector<ChainK>& K, const
     const int d = c->dim;
     const int64_t NK = int64_t(K.size());
     if (NK == 0 || int64_t(M.size()) != NK - 1) QND_FAIL(QND_EINVAL, "internal: malformed sandwich chain");
+    if (c->long1d) {
+        // one four-step sandwich per kinetic factor; the r-space work between them element-wise
+        auto point = [&](const Factor& f, int64_t lst, bool mask, const double* scale_dev) {
+            const void *tr = nullptr, *tc = nullptr;
+            const void* axc[MAX_DIM] = {nullptr, nullptr, nullptr};
+            set_factor(c, f, 0, lst, &tr, &tc, axc);
+            long_point(c, psi, tr, tc, axc[0], mask ? c->mask_dev[0].p : nullptr, scale_dev);
+        };
+        point(pre, pre_lst, false, pre_scale);
+        for (int64_t i = 0; i < NK; ++i) {
+            long_sandwich(c, psi, chain_spec(c, K[i], 0));
+            const ChainMid& m = i + 1 < NK ? M[i] : post;
+            point(m.f, m.lst, m.mask, nullptr);
+            if (m.red) grid_reduce(c, psi, *m.red);
+        }
+        return;
+    }
     auto finish = [&](PassSpec& ps) {
         set_factor(c, post.f, ps.axis, post.lst, &ps.epi_real, &ps.epi_cplx, nullptr);
         if (post.mask)
@@ -1050,7 +1230,7 @@ static void imag_steps(qnd_ctx* c, void* psi, int64_t nsteps, const double* pro_
 // nothing on it merges K(a_{2s-1}) with the next step's K(a_0).
 static void length_steps(qnd_ctx* c, void* psi, int64_t lst0, int64_t n, const RedFn& red_fn, bool masked) {
     if (n <= 0) return;
-    if (c->dim == 1 && n > 1 && (masked || red_fn)) {
+    if (c->dim == 1 && !c->long1d && n > 1 && (masked || red_fn)) {
         // 1-D chains carry boundary work only at their end
         for (int64_t k = 0; k < n; ++k)
             length_steps(c, psi, lst0 + k, 1, red_fn ? RedFn([&](int64_t, int ax) { return red_fn(k, ax); }) : RedFn(),
@@ -1142,6 +1322,17 @@ static void velocity_steps(qnd_ctx* c, void* psi, int64_t lst0, int64_t n, const
 }
 
 static void unitary_fft(qnd_ctx* c, void* psi, bool forward) {
+    if (c->long1d) {
+        const double s1 = 1.0 / std::sqrt(double(c->n1)), s2 = 1.0 / std::sqrt(double(c->n2));
+        if (forward) {
+            long_fft(c, psi, true, s1, s2);
+            long_reorder(c, psi, true);
+        } else {
+            long_reorder(c, psi, false);
+            long_fft(c, psi, false, s1, s2);
+        }
+        return;
+    }
     for (int ax : pass_order(c)) {
         PassSpec ps;
         ps.axis = ax;
@@ -1153,6 +1344,14 @@ static void unitary_fft(qnd_ctx* c, void* psi, bool forward) {
 }
 
 static const int64_t CHUNK = 128;
+
+// Steps per field chunk: CHUNK, or fewer where the chunk's per-step tables (s sub-steps x all axis
+// points) would pass 1 GiB (long 1-D axes).
+static int64_t chunk_steps(const qnd_ctx* c) {
+    const size_t per_step = size_t(c->s) * size_t(c->axtot) * c->elem();
+    const int64_t fit = int64_t((size_t(1) << 30) / std::max<size_t>(per_step, 1));
+    return std::max<int64_t>(1, std::min<int64_t>(CHUNK, fit));
+}
 
 // Run a chunk-wide chain (body) through a CUDA graph. The first run of a key goes directly (it
 // builds the tables the chain reads); the second captures it; later runs replay the graph, so the
@@ -1228,7 +1427,7 @@ static void run_realtime(qnd_ctx* c, void* psi, const double* field_host, const 
     const bool fused = all_rspace(items) && !velocity;  // velocity obs use A(t) -> evaluate per step
     const bool fused_v = all_rspace(items) && velocity;
     const bool masked = has_mask(c);
-    const int64_t ch_max = std::min<int64_t>(CHUNK, std::max<int64_t>(nsteps, 1));
+    const int64_t ch_max = std::min<int64_t>(chunk_steps(c), std::max<int64_t>(nsteps, 1));
     if (nv > 0) {
         c->obs_dev.ensure(size_t(ch_max + 1) * nv * sizeof(double));
         QND_CK(cudaMemsetAsync(c->obs_dev.p, 0, size_t(ch_max + 1) * nv * sizeof(double), c->stream));
@@ -1364,6 +1563,43 @@ static void scale_state(qnd_ctx* c, void* psi, const double* scale_dev) {
 
 static void set_device(qnd_ctx* c) { QND_CK(cudaSetDevice(c->device)); }
 
+// The tables of a long 1-D axis (see long_fft): pass twiddles for both virtual lengths, the
+// four-step twiddles W_N^{k1 n2} and their conjugates (FP32: stored as w - 1), slot momenta.
+static void build_long_axis(qnd_ctx* c) {
+    const int64_t N = c->nr[0];
+    c->long1d = true;
+    c->lg1 = std::max(4, c->lognr[0] - 12);  // n1 >= 16: the strided passes keep 16 values per thread
+    c->lg2 = c->lognr[0] - c->lg1;
+    c->n1 = int64_t(1) << c->lg1;
+    c->n2 = int64_t(1) << c->lg2;
+    build_twiddles(c, int(c->n1), c->tw_long[0]);
+    build_twiddles(c, int(c->n2), c->tw_long[1]);
+    std::vector<double> w(2 * size_t(N)), wc(2 * size_t(N));
+    const long double two_pi = 6.283185307179586476925286766559005768L;
+    for (int64_t k1 = 0; k1 < c->n1; ++k1)
+        for (int64_t m = 0; m < c->n2; ++m) {
+            const int64_t i = k1 * c->n2 + m;
+            const long double ang = two_pi * (long double)((k1 * m) & (N - 1)) / (long double)N;
+            const double sn = (double)sinl(ang);
+            double re;
+            if (c->fp64) {
+                re = (double)cosl(ang);
+            } else {
+                const long double sh = sinl(ang / 2);
+                re = (double)(-2 * sh * sh);
+            }
+            w[2 * i] = re;
+            w[2 * i + 1] = -sn;
+            wc[2 * i] = re;
+            wc[2 * i + 1] = sn;
+        }
+    upload_cplx(c, c->twf_long, w);
+    upload_cplx(c, c->twc_long, wc);
+    c->p_slot.resize(size_t(N));
+    for (int64_t i = 0; i < N; ++i) c->p_slot[i] = c->p[0][(i >> c->lg2) + ((i & (c->n2 - 1)) << c->lg1)];
+    upload_f64(c, c->p_slot_dev, c->p_slot);
+}
+
 static void build_context(qnd_ctx* c, int dim, const int64_t* nr, const double* dr, const char* integrator,
                           double dt, int precision) {
     if (dim < 1 || dim > MAX_DIM) QND_FAIL(QND_EINVAL, "dimension %d not in 1..3", dim);
@@ -1371,10 +1607,13 @@ static void build_context(qnd_ctx* c, int dim, const int64_t* nr, const double* 
     c->fp64 = precision == QND_FP64;
     c->dim = dim;
     c->n = 1;
+    // one pass handles an axis of up to 4096 points; a 1-D grid goes up to 2^24 points in four steps
+    const int64_t nmax = dim == 1 ? LONG_AXIS_MAX : 4096;
     for (int j = 0; j < dim; ++j) {
-        if (nr[j] < 2 || nr[j] > 4096 || (nr[j] & (nr[j] - 1)))
-            QND_FAIL(nr[j] > 4096 ? QND_EUNSUPPORTED : QND_EINVAL,
-                     "NR[%d]=%lld: must be a power of 2 between 2 and 4096", j, (long long)nr[j]);
+        if (nr[j] < 2 || nr[j] > nmax || (nr[j] & (nr[j] - 1)))
+            QND_FAIL(nr[j] > nmax ? QND_EUNSUPPORTED : QND_EINVAL,
+                     "NR[%d]=%lld: must be a power of 2 between 2 and %lld%s", j, (long long)nr[j], (long long)nmax,
+                     dim == 1 ? "" : " (axes longer than 4096 are built for 1-D grids)");
         if (!(dr[j] > 0)) QND_FAIL(QND_EINVAL, "DR[%d] must be positive", j);
         c->nr[j] = nr[j];
         c->dr[j] = dr[j];
@@ -1441,7 +1680,11 @@ static void build_context(qnd_ctx* c, int dim, const int64_t* nr, const double* 
     }
     upload_f64(c, c->r_dev, rall);
     upload_f64(c, c->p_dev, pall);
-    for (int j = 0; j < dim; ++j) build_twiddles(c, j);
+    if (dim == 1 && nr[0] > 4096) {
+        build_long_axis(c);
+        return;
+    }
+    for (int j = 0; j < dim; ++j) build_twiddles(c, int(c->nr[j]), c->tw[j]);
 }
 
 // Named potentials as functions of |r| (meshgrid.c:137-153) and their radial derivative dV/dr.
@@ -1769,8 +2012,9 @@ int qnd_step_length(qnd_ctx* ctx, void* psi_p_dev, const double* E_host, int64_t
     QND_NEED(E_host);
     set_device(ctx);
     unitary_fft(ctx, psi_p_dev, false);
-    for (int64_t c0 = 0; c0 < nsteps; c0 += CHUNK) {
-        const int64_t ch = std::min(CHUNK, nsteps - c0);
+    const int64_t chunk = chunk_steps(ctx);
+    for (int64_t c0 = 0; c0 < nsteps; c0 += chunk) {
+        const int64_t ch = std::min(chunk, nsteps - c0);
         upload_field_chunk(ctx, E_host + size_t(c0) * ctx->s * ctx->dim, ch, false);
         length_steps(ctx, psi_p_dev, 0, ch, RedFn(), false);
     }
@@ -1786,8 +2030,9 @@ int qnd_step_velocity(qnd_ctx* ctx, void* psi_dev, const double* A_host, int64_t
     if (nsteps <= 0) return QND_OK;
     QND_NEED(A_host);
     set_device(ctx);
-    for (int64_t c0 = 0; c0 < nsteps; c0 += CHUNK) {
-        const int64_t ch = std::min(CHUNK, nsteps - c0);
+    const int64_t chunk = chunk_steps(ctx);
+    for (int64_t c0 = 0; c0 < nsteps; c0 += chunk) {
+        const int64_t ch = std::min(chunk, nsteps - c0);
         upload_field_chunk(ctx, A_host + size_t(c0) * ctx->s * ctx->dim, ch, true);
         velocity_steps(ctx, psi_dev, 0, ch, nullptr, false);
     }
@@ -1884,15 +2129,16 @@ int qnd_run_length_dev(qnd_ctx* ctx, void* psi_r_dev, const double* E_dev, int64
     const double zero[MAX_DIM] = {0, 0, 0};
     // observables that are r-space reductions of one descriptor: chunk-wide chains
     const bool chain = nv == 0 || (fused && rspace_red(ctx, items, obs_dev, 0).size() <= 1);
-    for (int64_t c0 = 0; c0 < nsteps; c0 += CHUNK) {
-        const int64_t ch = std::min(CHUNK, nsteps - c0);
+    const int64_t chunk = chunk_steps(ctx);
+    for (int64_t c0 = 0; c0 < nsteps; c0 += chunk) {
+        const int64_t ch = std::min(chunk, nsteps - c0);
         build_field_tables(ctx, E_dev + size_t(c0) * ctx->s * ctx->dim, ch, false);
         if (chain) {
             // rows are staged in the context's buffer (fixed addresses, so that a captured chain
             // replays for every chunk), then copied to obs_dev
             double* stage = nullptr;
             if (nv > 0) {
-                ctx->obs_dev.ensure(size_t(CHUNK) * nv * sizeof(double));
+                ctx->obs_dev.ensure(size_t(chunk) * nv * sizeof(double));
                 stage = ctx->obs_dev.as<double>();
             }
             RedFn rf;

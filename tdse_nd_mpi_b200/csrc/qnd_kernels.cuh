@@ -100,4 +100,26 @@ template <typename R>
 void launch_ped(const SpectraArgs& a, const cplx_t<R>* psi_p, double* partials, double* out, cudaStream_t st);
 template <typename R> void launch_pmd(const SpectraArgs& a, const cplx_t<R>* psi_p, double* out, cudaStream_t st);
 
+// Axes longer than one pass handles (1-D, N = N1 N2): the four-step transform over the virtual
+// N1 x N2 grid (index n1 N2 + n2), see long_fft in qnd_engine.cu. Slot k1 N2 + k2 of its output
+// holds frequency k1 + N1 k2.
+struct LongArgs {
+    long long n;          // N
+    int log2n1, log2n2;
+};
+// psi[k1 N2 + n2] times the stored twiddle w[k1 N2 + n2] (W_N^{k1 n2}), or its conjugate
+template <typename R> void launch_long_twiddle(const LongArgs& a, cplx_t<R>* psi, const cplx_t<R>* w, int conj,
+                                               cudaStream_t st);
+// to_natural: out[k1 + N1 k2] = in[k1 N2 + k2]; otherwise the inverse permutation
+template <typename R> void launch_long_transpose(const LongArgs& a, const cplx_t<R>* in, cplx_t<R>* out, int to_natural,
+                                                 cudaStream_t st);
+// Point-wise factors of a 1-D state in natural order: real table, complex table, per-axis complex
+// table, real per-axis table (the mask), device scalar; any may be null.
+template <typename R> void launch_point_factors(long long n, cplx_t<R>* psi, const R* tr, const cplx_t<R>* tc,
+                                                const cplx_t<R>* pc, const R* pr, const double* scale_dev,
+                                                cudaStream_t st);
+// dst += vtab * src (H psi = T psi + V psi)
+template <typename R> void launch_add_potential(long long n, cplx_t<R>* dst, const cplx_t<R>* src, const double* vtab,
+                                                cudaStream_t st);
+
 }  // namespace qnd

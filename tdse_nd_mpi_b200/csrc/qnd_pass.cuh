@@ -68,6 +68,8 @@ template <typename R> struct PassArgs {
     const V* pro_cplx;
     const double* pro_scale_dev;
     const V* spec;
+    int spec_full;               // spec is a full-grid table in line-major order (one row per line),
+                                 // not one row shared by every line (the long-axis four-step pass)
     const V* spec2;              // PM_DOUBLE: the second sandwich's spectral factors
     const R* mid_real;           // PM_DOUBLE: r-space factors between the two sandwiches
     const V* mid_cplx;
@@ -456,7 +458,7 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
     } else {
         // SANDWICH / DOUBLE / APPLY: spectral multiply, inverse transform
         if (a.spec) {
-            const V* __restrict__ sp = a.spec;
+            const V* __restrict__ sp = a.spec + (a.spec_full ? lbase : 0ll);
 #pragma unroll
             for (int u = 0; u < E; ++u)
                 v[u] = fmul_spec<L>(v[u], __ldg(sp + tid + u * T), key0 + uint32_t(tid + u * T), u == 0 || u == E - 1);
