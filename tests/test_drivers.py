@@ -144,11 +144,12 @@ def _text_table(path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("gauge", ["length", "velocity"])
-def test_real_driver_outputs_match_reference_executable(driver, tmp_path, gauge):
+@pytest.mark.parametrize("gauge,nr", [("length", 512), ("velocity", 512), ("length", 16384)])
+def test_real_driver_outputs_match_reference_executable(driver, tmp_path, gauge, nr):
     """QuantumND_real end to end (two-state superposition read from output.imag onto a larger grid,
     two laser modes, CAP, observables every step, PED/PMD/wavefunction) against the reference's
-    executable on the same inputs: every output file."""
+    executable on the same inputs: every output file. NR 16384: a 1-D axis past one pass (the
+    four-step transform)."""
     from oracle import oracle as O
 
     if not (os.path.exists(REF_IMAG) and os.path.exists(REF_REAL)):
@@ -161,7 +162,7 @@ def test_real_driver_outputs_match_reference_executable(driver, tmp_path, gauge)
         d = tmp_path / who
         d.mkdir()
         (d / "output.imag").write_bytes((seed / "output.imag").read_bytes())
-        (d / "params.real").write_text(PARAMS_REAL.format(gauge=gauge))
+        (d / "params.real").write_text(PARAMS_REAL.format(gauge=gauge).replace("NR\t\t512", f"NR\t\t{nr}"))
         r = subprocess.run([exe, "params.real"], cwd=d, capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, (who, r.stdout[-2000:], r.stderr[-2000:])
         out[who] = d
