@@ -160,6 +160,40 @@ int qnd_final_spectra(qnd_ctx *ctx, const void *psi_r_dev, double r_mask_min, do
 int qnd_observables_rspace_noalloc(qnd_ctx *ctx, const void *psi_r_dev, int nobs, const char *const *names,
                                    double *out_dev);
 
+/* ---- laser field on the device: replaces Initialize_field_vectors (integrators.c:74-101) and
+ *      Field_vectors (parameters.c:899-949).
+ * One mode of the field, as the reference holds it after parameters.c:805-810: frequency
+ * omega = 45.5637639947958 / LAMBDA, amplitude F0 = 5.33803e-9 sqrt(INTENSITY), ELLIPTICITY, CEP,
+ * DELAY, DURATION, and the envelope (QND_ENV_*: "constant", "trapz", "cos2", "cos4"). */
+#define QND_ENV_CONSTANT 0
+#define QND_ENV_TRAPZ 1
+#define QND_ENV_COS2 2
+#define QND_ENV_COS4 3
+typedef struct {
+    double frequency, amplitude, ellipticity, cep, delay, duration;
+    int envelope;
+} qnd_laser_mode;
+
+/* E and A summed over the modes (components 0 and, for dim >= 2, 1; the rest 0) at the
+ * integrator's sub-step times of steps 0 .. nsteps-1: t = i dt + as[0], then
+ * t += as[2j+1] + as[2j+2] between sub-steps j and j+1 (integrators.c:90-99). E_out and A_out are
+ * [nsteps][s][dim] (the F.E / F.A layout, ready for qnd_run_length / qnd_run_velocity);
+ * alpha_out is [nsteps][dim] = A(i dt), the velocity-gauge observables' shift (QuantumND_real.c:173).
+ * Any output may be NULL. on_device = 0: host arrays (the samples are computed on the device and
+ * copied back; synchronises); 1: device arrays, filled asynchronously on the context's stream
+ * (for qnd_run_length_dev). */
+int qnd_field_samples(qnd_ctx *ctx, int nmodes, const qnd_laser_mode *modes, int64_t nsteps, double *E_out,
+                      double *A_out, double *alpha_out, int on_device);
+
+/* ---- initial state on the device: the centring and superposition of Read_wavefunction_MPI
+ *      (io_functions.c:292-459).
+ * psi_dev <- (accumulate ? psi_dev : 0) + coeff * src, where src (host, complex128) is a state on a
+ * grid of nr_src[dim] points with this grid's spacing, placed so that point i_j of axis j lands on
+ * i_j + (nr[j] - nr_src[j]) / 2; points that fall outside this grid are dropped. Call once per
+ * OUTPUT_IMAG state with accumulate = 0 for the first. */
+int qnd_state_embed(qnd_ctx *ctx, void *psi_dev, const double *src_host, const int64_t *nr_src, double coeff_re,
+                    double coeff_im, int accumulate);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,7 +55,18 @@ SIGNATURES = {
     "qnd_energies": ([_vp, _vp, C.c_int, _dp], C.c_int),
     "qnd_observables_rspace_noalloc": ([_vp, _vp, C.c_int, _names, _vp], C.c_int),
     "qnd_final_spectra": ([_vp, _vp, C.c_double, C.c_double, _dp, C.c_double, C.c_int, _dp, _i64p, _dp], C.c_int),
+    "qnd_field_samples": ([_vp, C.c_int, _vp, _i64, _vp, _vp, _vp, C.c_int], C.c_int),
+    "qnd_state_embed": ([_vp, _vp, _dp, _i64p, C.c_double, C.c_double, C.c_int], C.c_int),
 }
+
+QND_ENV = {"constant": 0, "trapz": 1, "cos2": 2, "cos4": 3}
+
+
+class LaserMode(C.Structure):
+    """qnd_laser_mode: one mode as the reference holds it after parameters.c:805-810."""
+
+    _fields_ = [("frequency", C.c_double), ("amplitude", C.c_double), ("ellipticity", C.c_double),
+                ("cep", C.c_double), ("delay", C.c_double), ("duration", C.c_double), ("envelope", C.c_int)]
 
 _lib = None
 

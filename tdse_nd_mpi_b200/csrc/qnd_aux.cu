@@ -261,6 +261,115 @@ template <typename R> void launch_pmd(const SpectraArgs& a, const cplx_t<R>* psi
     pmd_kernel<R><<<(int)nb, 256, 0, st>>>(a, psi_p, out);
 }
 
+// ---- laser field samples (integrators.c:74-101, parameters.c:899-949) -------------
+
+// E(t) and A(t) summed over the modes: envelope f(ts) and its derivative df, ts = t - delay,
+// A = F0 f (cos, xi sin)(w ts + cep) / w, E = -dA/dt (parameters.c:911-946).
+__device__ void field_at(const FieldSampleArgs& a, double t, double* A, double* E) {
+    const double pi = 3.14159265358979323846;
+    for (int j = 0; j < a.dim; ++j) A[j] = E[j] = 0.0;
+    for (int m = 0; m < a.nmodes; ++m) {
+        const FieldMode& md = a.mode[m];
+        const double w = md.w, ts = t - md.delay, tau = md.tau;
+        double f = 0.0, df = 0.0;
+        if (md.env == ENV_CONSTANT) {
+            f = 1.0;
+        } else if (md.env == ENV_TRAPZ) {
+            const double tr = 2. * 2. * pi / w;
+            const double up = (ts >= 0. && ts <= tr) ? 1. : 0., flat = (ts > tr && ts < tau - tr) ? 1. : 0.,
+                         down = (ts >= tau - tr && ts <= tau) ? 1. : 0.;
+            const double s1 = sin(.5 * pi * ts / tr), s2 = sin(.5 * pi * (ts - tau) / tr);
+            f = pow(s1, 4) * up + flat + pow(s2, 4) * down;
+            df = pi / tr * (pow(s1, 2) * sin(pi * ts / tr) * up + pow(s2, 2) * sin(pi * (ts - tau) / tr) * down);
+        } else {
+            const double on = (ts >= 0. && ts <= tau) ? 1. : 0.;
+            const double sn = sin(pi * ts / tau);
+            if (md.env == ENV_COS2) {
+                f = pow(sn, 2) * on;
+                df = pi * sin(2. * pi * ts / tau) / tau * on;
+            } else {
+                f = pow(sn, 4) * on;
+                df = 4. * pi * cos(pi * ts / tau) * pow(sn, 3) / tau * on;
+            }
+        }
+        double sp, cp;
+        sincos(w * ts + md.cep, &sp, &cp);
+        E[0] += -md.F0 * (df * cp - f * w * sp) / w;
+        A[0] += md.F0 * f * cp / w;
+        if (a.dim >= 2) {
+            E[1] += -md.F0 * md.xi * (df * sp + f * w * cp) / w;
+            A[1] += md.F0 * md.xi * f * sp / w;
+        }
+    }
+}
+
+// One thread per (step i, slot j): j < s the sub-step samples, j == s the step-start alpha.
+__global__ void __launch_bounds__(256) field_samples_kernel(const __grid_constant__ FieldSampleArgs a, double* E,
+                                                            double* A, double* alpha) {
+    const long long total = a.nsteps * (a.s + 1);
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += (long long)gridDim.x * blockDim.x) {
+        const long long i = q / (a.s + 1);
+        const int j = int(q - i * (a.s + 1));
+        double av[MAX_DIM], ev[MAX_DIM];
+        if (j == a.s) {
+            if (!alpha) continue;
+            field_at(a, __dmul_rn(double(i), a.dt), av, ev);
+            for (int k = 0; k < a.dim; ++k) alpha[i * a.dim + k] = av[k];
+            continue;
+        }
+        if (!E && !A) continue;
+        // the sub-step time accumulated as in integrators.c:90-99
+        double t = __dadd_rn(__dmul_rn(double(i), a.dt), a.as[0]);
+        for (int jj = 0; jj < j; ++jj) t = __dadd_rn(t, __dadd_rn(a.as[2 * jj + 1], a.as[2 * jj + 2]));
+        field_at(a, t, av, ev);
+        const long long o = (i * a.s + j) * a.dim;
+        for (int k = 0; k < a.dim; ++k) {
+            if (E) E[o + k] = ev[k];
+            if (A) A[o + k] = av[k];
+        }
+    }
+}
+
+void launch_field_samples(const FieldSampleArgs& a, double* E, double* A, double* alpha, cudaStream_t st) {
+    const long long total = a.nsteps * (a.s + 1);
+    long long nb = (total + 255) / 256;
+    if (nb > 148 * 16) nb = 148 * 16;
+    if (nb < 1) nb = 1;
+    field_samples_kernel<<<int(nb), 256, 0, st>>>(a, E, A, alpha);
+}
+
+// ---- initial state: centring + superposition (io_functions.c:292-459) -------------
+
+template <typename R>
+__global__ void __launch_bounds__(256) embed_kernel(const __grid_constant__ EmbedArgs a, const double2* src,
+                                                    cplx_t<R>* psi) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n_src; i += (long long)gridDim.x * blockDim.x) {
+        long long idx = i, dst = 0, mult = 1;
+        bool ok = true;
+        for (int j = a.dim - 1; j >= 0; --j) {
+            const long long ij = idx % a.nr_src[j] + a.off[j];
+            idx /= a.nr_src[j];
+            if (ij < 0 || ij >= a.nr[j]) ok = false;
+            dst += ij * mult;
+            mult *= a.nr[j];
+        }
+        if (!ok) continue;
+        const double2 v = src[i];
+        // c * v rounded per operation (no contraction), as a C99 complex product
+        const double re = __dsub_rn(__dmul_rn(a.cr, v.x), __dmul_rn(a.ci, v.y));
+        const double im = __dadd_rn(__dmul_rn(a.cr, v.y), __dmul_rn(a.ci, v.x));
+        const cplx_t<R> p = psi[dst];
+        psi[dst] = cplx_t<R>{R(__dadd_rn(double(p.x), re)), R(__dadd_rn(double(p.y), im))};
+    }
+}
+
+template <typename R> void launch_embed(const EmbedArgs& a, const double2* src, cplx_t<R>* psi, cudaStream_t st) {
+    long long nb = (a.n_src + 255) / 256;
+    if (nb > 148 * 16) nb = 148 * 16;
+    if (nb < 1) nb = 1;
+    embed_kernel<R><<<int(nb), 256, 0, st>>>(a, src, psi);
+}
+
 // ---- axes longer than one pass: the four-step pieces (qnd_engine.cu, long_fft) -------
 
 template <typename R>
@@ -343,7 +452,8 @@ template <typename R> void launch_add_potential(long long n, cplx_t<R>* dst, con
     template void launch_long_transpose<R>(const LongArgs&, const cplx_t<R>*, cplx_t<R>*, int, cudaStream_t); \
     template void launch_point_factors<R>(long long, cplx_t<R>*, const R*, const cplx_t<R>*, const cplx_t<R>*, \
                                           const R*, const double*, cudaStream_t);                          \
-    template void launch_add_potential<R>(long long, cplx_t<R>*, const cplx_t<R>*, const double*, cudaStream_t);
+    template void launch_add_potential<R>(long long, cplx_t<R>*, const cplx_t<R>*, const double*, cudaStream_t); \
+    template void launch_embed<R>(const EmbedArgs&, const double2*, cplx_t<R>*, cudaStream_t);
 QND_INST(double)
 QND_INST(float)
 #undef QND_INST

@@ -150,6 +150,7 @@ struct qnd_ctx {
     DevBuf field_dev, field_tab, wtab_dev[MAX_DIM], spec_tmp[MAX_DIM];
     DevBuf scratch_a, scratch_b;
     DevBuf spec_rank, spec_partials, spec_out;  // final spectra: per-axis ranks, partial sums, results
+    DevBuf field_out, embed_src;                // qnd_field_samples host-output staging; qnd_state_embed source
 
     // A 1-D axis longer than one pass handles: N = n1 n2 (n1 >= 16, n2 <= 4096) as a virtual
     // n1 x n2 grid transformed in four steps (long_fft). tw_long[v]: the stage twiddles of the
@@ -2332,6 +2333,84 @@ int qnd_final_spectra(qnd_ctx* ctx, const void* psi_r_dev, double r_mask_min, do
                                ctx->stream));
         QND_CK(cudaStreamSynchronize(ctx->stream));
     }
+    QND_API_END
+}
+
+int qnd_field_samples(qnd_ctx* ctx, int nmodes, const qnd_laser_mode* modes, int64_t nsteps, double* E_out,
+                      double* A_out, double* alpha_out, int on_device) {
+    using namespace qnd;
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    if (nmodes < 0 || nmodes > MAX_MODES) QND_FAIL(QND_EUNSUPPORTED, "%d laser modes: this build takes 0 to %d", nmodes, MAX_MODES);
+    if (nmodes > 0) QND_NEED(modes);
+    if (nsteps < 0) QND_FAIL(QND_EINVAL, "nsteps %lld < 0", (long long)nsteps);
+    if (nsteps == 0 || (!E_out && !A_out && !alpha_out)) return QND_OK;
+    set_device(ctx);
+    FieldSampleArgs a{};
+    for (int m = 0; m < nmodes; ++m) {
+        const qnd_laser_mode& md = modes[m];
+        if (md.envelope < QND_ENV_CONSTANT || md.envelope > QND_ENV_COS4)
+            QND_FAIL(QND_EINVAL, "Unknown envelope code %d (mode %d)", md.envelope, m);
+        a.mode[m] = FieldMode{md.frequency, md.amplitude, md.ellipticity, md.cep, md.delay, md.duration, md.envelope};
+    }
+    a.nmodes = nmodes;
+    a.dim = ctx->dim;
+    a.s = ctx->s;
+    a.nsteps = nsteps;
+    a.dt = ctx->dt;
+    for (int k = 0; k < 2 * ctx->s; ++k) a.as[k] = ctx->as[k];
+    const size_t nsub = size_t(nsteps) * ctx->s * ctx->dim, nal = size_t(nsteps) * ctx->dim;
+    if (on_device) {
+        launch_field_samples(a, E_out, A_out, alpha_out, ctx->stream);
+        ctx->kernels_launched++;
+        QND_CK(cudaGetLastError());
+        return QND_OK;
+    }
+    ctx->field_out.ensure((2 * nsub + nal) * sizeof(double));
+    double* dE = ctx->field_out.as<double>();
+    double* dA = dE + nsub;
+    double* dal = dA + nsub;
+    launch_field_samples(a, E_out ? dE : nullptr, A_out ? dA : nullptr, alpha_out ? dal : nullptr, ctx->stream);
+    ctx->kernels_launched++;
+    QND_CK(cudaGetLastError());
+    if (E_out) QND_CK(cudaMemcpyAsync(E_out, dE, nsub * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (A_out) QND_CK(cudaMemcpyAsync(A_out, dA, nsub * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (alpha_out) QND_CK(cudaMemcpyAsync(alpha_out, dal, nal * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    QND_CK(cudaStreamSynchronize(ctx->stream));
+    QND_API_END
+}
+
+int qnd_state_embed(qnd_ctx* ctx, void* psi_dev, const double* src_host, const int64_t* nr_src, double coeff_re,
+                    double coeff_im, int accumulate) {
+    using namespace qnd;
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi_dev);
+    QND_NEED(src_host);
+    QND_NEED(nr_src);
+    EmbedArgs a{};
+    a.dim = ctx->dim;
+    a.n_src = 1;
+    for (int j = 0; j < ctx->dim; ++j) {
+        if (nr_src[j] < 1) QND_FAIL(QND_EINVAL, "source grid NR[%d]=%lld < 1", j, (long long)nr_src[j]);
+        a.nr_src[j] = nr_src[j];
+        a.nr[j] = ctx->nr[j];
+        a.off[j] = (ctx->nr[j] - nr_src[j]) / 2;  // C division, as io_functions.c's centring offset
+        a.n_src *= nr_src[j];
+    }
+    a.cr = coeff_re;
+    a.ci = coeff_im;
+    set_device(ctx);
+    if (!accumulate) QND_CK(cudaMemsetAsync(psi_dev, 0, size_t(ctx->n) * ctx->elem(), ctx->stream));
+    ctx->embed_src.ensure(size_t(a.n_src) * 16);
+    QND_CK(cudaMemcpyAsync(ctx->embed_src.p, src_host, size_t(a.n_src) * 16, cudaMemcpyHostToDevice, ctx->stream));
+    if (ctx->fp64)
+        launch_embed<double>(a, ctx->embed_src.as<double2>(), static_cast<double2*>(psi_dev), ctx->stream);
+    else
+        launch_embed<float>(a, ctx->embed_src.as<double2>(), static_cast<float2*>(psi_dev), ctx->stream);
+    ctx->kernels_launched++;
+    QND_CK(cudaGetLastError());
+    QND_CK(cudaStreamSynchronize(ctx->stream));  // the caller may release src_host on return
     QND_API_END
 }
 

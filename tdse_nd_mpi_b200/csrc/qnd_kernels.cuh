@@ -73,6 +73,34 @@ struct FieldTableArgs {
 };
 template <typename R> void launch_field_tables(const FieldTableArgs& a, cplx_t<R>* out, cudaStream_t st);
 
+// Laser field samples at the integrator's sub-step times (Initialize_field_vectors,
+// integrators.c:74-101) from the modes of Field_vectors (parameters.c:899-949).
+constexpr int MAX_MODES = 16;
+enum : int { ENV_CONSTANT = 0, ENV_TRAPZ = 1, ENV_COS2 = 2, ENV_COS4 = 3 };
+struct FieldMode {
+    double w, F0, xi, cep, delay, tau;
+    int env;
+};
+struct FieldSampleArgs {
+    FieldMode mode[MAX_MODES];
+    int nmodes, dim, s;
+    long long nsteps;
+    double dt;
+    double as[20];
+};
+// E, A: [nsteps][s][dim] at the sub-step times; alpha: [nsteps][dim] = A(i dt). Any may be null.
+void launch_field_samples(const FieldSampleArgs& a, double* E, double* A, double* alpha, cudaStream_t st);
+
+// The centring + superposition of Read_wavefunction_MPI (io_functions.c:292-459):
+// psi[i + off] (+)= c src[i] over the source grid, points outside psi's grid dropped.
+struct EmbedArgs {
+    long long n_src;
+    int dim;
+    long long nr_src[MAX_DIM], nr[MAX_DIM], off[MAX_DIM];
+    double cr, ci;
+};
+template <typename R> void launch_embed(const EmbedArgs& a, const double2* src, cplx_t<R>* psi, cudaStream_t st);
+
 // Per-axis tables that depend on a runtime shift alpha:
 //   mode 0: w[k] = p[k] + alpha (double)            dipole_v weights
 //   mode 1: spec[k] = (p[k] + alpha) / N (complex)   Lz operator

@@ -345,45 +345,33 @@ static void print_params(const RealParams *P) {
     fflush(stdout);
 }
 
-/* Field_vectors (parameters.c:899-949): E(t) and A(t) summed over the modes, components 0 and 1. */
-static void field_vectors(const RealParams *P, double t, double *A, double *E) {
-    for (int j = 0; j < P->dim; ++j) E[j] = A[j] = 0.;
-    for (int m = 0; m < P->nmodes; ++m) {
-        const double w = P->frequency[m], F0 = P->amplitude[m], xi = P->ellipticity[m], tau = P->duration[m];
-        const double ph = P->cep[m], ts = t - P->delay[m];
-        double f = 0., df = 0.;
-        const char *env = P->envelope[m];
-        if (!strcmp(env, "constant")) {
-            f = 1.;
-            df = 0.;
-        } else if (!strcmp(env, "trapz")) {
-            const double tr = 2. * 2. * M_PI / w;
-            const int up = ts >= 0. && ts <= tr, flat = ts > tr && ts < tau - tr, down = ts >= tau - tr && ts <= tau;
-            f = pow(sin(.5 * M_PI * ts / tr), 4) * up + flat + pow(sin(.5 * M_PI * (ts - tau) / tr), 4) * down;
-            df = M_PI / tr * (pow(sin(.5 * M_PI * ts / tr), 2) * sin(M_PI * ts / tr) * up +
-                              pow(sin(.5 * M_PI * (ts - tau) / tr), 2) * sin(M_PI * (ts - tau) / tr) * down);
-        } else if (!strcmp(env, "cos2")) {
-            const int on = ts >= 0. && ts <= tau;
-            f = pow(sin(M_PI * ts / tau), 2) * on;
-            df = M_PI * sin(2. * M_PI * ts / tau) / tau * on;
-        } else if (!strcmp(env, "cos4")) {
-            const int on = ts >= 0. && ts <= tau;
-            f = pow(sin(M_PI * ts / tau), 4) * on;
-            df = 4. * M_PI * cos(M_PI * ts / tau) * pow(sin(M_PI * ts / tau), 3) / tau * on;
-        } else {
-            printf("\nUnknown envelope: %s\n", env);
+/* The field modes for qnd_field_samples, which evaluates Field_vectors (parameters.c:899-949) on the
+ * device; an unknown envelope name stops the run as Field_vectors does. */
+static qnd_laser_mode *laser_modes(const RealParams *P) {
+    qnd_laser_mode *m = calloc((size_t)P->nmodes + 1, sizeof(qnd_laser_mode));
+    static const char *const env[] = {"constant", "trapz", "cos2", "cos4"};
+    for (int k = 0; k < P->nmodes; ++k) {
+        m[k].frequency = P->frequency[k];
+        m[k].amplitude = P->amplitude[k];
+        m[k].ellipticity = P->ellipticity[k];
+        m[k].cep = P->cep[k];
+        m[k].delay = P->delay[k];
+        m[k].duration = P->duration[k];
+        m[k].envelope = -1;
+        for (int e = 0; e < 4; ++e)
+            if (!strcmp(P->envelope[k], env[e])) m[k].envelope = e;
+        if (m[k].envelope < 0) {
+            printf("\nUnknown envelope: %s\n", P->envelope[k]);
             fail("Error with the envelope name");
         }
-        E[0] += -F0 * (df * cos(w * ts + ph) - f * w * sin(w * ts + ph)) / w;
-        if (P->dim >= 2) E[1] += -F0 * xi * (df * sin(w * ts + ph) + f * w * cos(w * ts + ph)) / w;
-        A[0] += F0 * f * cos(w * ts + ph) / w;
-        if (P->dim >= 2) A[1] += F0 * xi * f * sin(w * ts + ph) / w;
     }
+    return m;
 }
 
-/* Read_wavefunction_MPI (io_functions.c:292-459): the chosen OUTPUT_IMAG states, centred on the
- * (possibly larger or smaller) real-time grid, superposed with the normalised coefficients. */
-static void read_initial_state(const RealParams *P, double complex *psi, int64_t n) {
+/* Read_wavefunction_MPI (io_functions.c:292-459): the chosen OUTPUT_IMAG states are read here and
+ * centred on the (possibly larger or smaller) real-time grid and superposed with the normalised
+ * coefficients on the device (qnd_state_embed). */
+static void read_initial_state(const RealParams *P, qnd_ctx *q, void *psi_dev) {
     FILE *f = fopen(P->output_imag, "rb");
     if (!f) fail("Rank 0: Error opening the output of the imaginary time propagation");
     char key[64];
@@ -398,29 +386,15 @@ static void read_initial_state(const RealParams *P, double complex *psi, int64_t
         }
     }
     if (off == 0) fail("Rank 0: Error: Could not find 'PSI' marker in file.");
-    int64_t n_imag = 1, off_c[3] = {0, 0, 0};
-    for (int j = 0; j < P->dim; ++j) {
-        n_imag *= P->nr_imag[j];
-        off_c[j] = (P->nr[j] - P->nr_imag[j]) / 2;
-    }
-    double complex *buf = malloc(sizeof(double complex) * (size_t)n_imag);
-    memset(psi, 0, sizeof(double complex) * (size_t)n);
+    int64_t n_imag = 1;
+    for (int j = 0; j < P->dim; ++j) n_imag *= P->nr_imag[j];
+    double complex *buf = calloc((size_t)n_imag, sizeof(double complex));
+    if (P->nstates < 1) CK(qnd_state_embed(q, psi_dev, (const double *)buf, P->nr_imag, 0., 0., 0));  /* zero state */
     for (int k = 0; k < P->nstates; ++k) {
         if (fseek(f, off + (long)(P->j_states[k] - 1) * (long)n_imag * (long)sizeof(double complex), SEEK_SET) != 0 ||
             fread(buf, sizeof(double complex), (size_t)n_imag, f) != (size_t)n_imag)
             fail("Rank 0: MPI Read Error during chunking");
-        for (int64_t i = 0; i < n_imag; ++i) {
-            int64_t idx = i, dst = 0, mult = 1;
-            int ok = 1;
-            for (int j = P->dim - 1; j >= 0; --j) {
-                const int64_t ij = idx % P->nr_imag[j] + off_c[j];
-                idx /= P->nr_imag[j];
-                if (ij < 0 || ij >= P->nr[j]) ok = 0;
-                dst += ij * mult;
-                mult *= P->nr[j];
-            }
-            if (ok) psi[dst] += P->coeffs[k] * buf[i];
-        }
+        CK(qnd_state_embed(q, psi_dev, (const double *)buf, P->nr_imag, creal(P->coeffs[k]), cimag(P->coeffs[k]), k > 0));
     }
     free(buf);
     fclose(f);
@@ -451,11 +425,14 @@ int main(int argc, char **argv) {
     double *A = calloc((size_t)(nt * s * P.dim) + 1, sizeof(double));
     FILE *fe = fopen("electric_field.real", "w"), *fa = fopen("vector_potential.real", "w");
     if (!fe || !fa) fail("Error opening the files of the vector potential and the laser electric field.");
+    double *alpha = calloc((size_t)(nt * P.dim) + 1, sizeof(double));
+    qnd_laser_mode *modes = laser_modes(&P);
+    CK(qnd_field_samples(q, P.nmodes, modes, nt, E, A, alpha, 0));
+    free(modes);
     for (int64_t i = 0; i < nt; ++i) {
         double t = (double)i * P.dt + as[0];
         const int64_t ind = i * P.dim * s;
         for (int j = 0; j < s; ++j) {
-            field_vectors(&P, t, &A[ind + j * P.dim], &E[ind + j * P.dim]);
             fprintf(fe, "%16.15f ", t);
             fprintf(fa, "%16.15f ", t);
             for (int k = 0; k < P.dim; ++k) {
@@ -496,10 +473,9 @@ int main(int argc, char **argv) {
     CK(qnd_set_cap(q, P.cap[0], P.cap[1]));
     printf("\n# Initialization of the wave function\n");
     double complex *psi = malloc(sizeof(double complex) * (size_t)n);
-    read_initial_state(&P, psi, n);
     void *psi_dev = NULL;
     CK(qnd_state_alloc(q, 1, &psi_dev));
-    CK(qnd_state_upload(q, psi_dev, (const double *)psi));
+    read_initial_state(&P, q, psi_dev);
 
     printf("\n# Real-time propagation\n");
     clock_t c0 = clock();
@@ -509,12 +485,7 @@ int main(int argc, char **argv) {
     CK(qnd_observable_count(q, P.nobs, names, &nv));
     double *rows = calloc((size_t)(nt * (nv > 0 ? nv : 1)), sizeof(double));
     if (!strcmp(P.gauge, "velocity")) {
-        double *alpha = calloc((size_t)(nt * P.dim) + 1, sizeof(double));
-        double *ebuf = calloc((size_t)P.dim, sizeof(double));
-        for (int64_t i = 0; i < nt; ++i) field_vectors(&P, (double)i * P.dt, &alpha[i * P.dim], ebuf);
         CK(qnd_run_velocity(q, psi_dev, A, alpha, nt, P.nobs, names, rows));
-        free(alpha);
-        free(ebuf);
     } else if (!strcmp(P.gauge, "length")) {
         CK(qnd_run_length(q, psi_dev, E, nt, P.nobs, names, rows));
     } else {
@@ -599,6 +570,7 @@ int main(int argc, char **argv) {
     free(rows);
     free(E);
     free(A);
+    free(alpha);
     free(names);
     return 0;
 }

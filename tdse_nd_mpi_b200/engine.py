@@ -304,3 +304,45 @@ class Grid:
         out = np.zeros(n)
         check(lib().qnd_energies(self.h, C.c_void_p(_ptr_of(psi_r)), int(n), _dptr(out)))
         return out
+
+    # -- laser field and initial state on the device
+    @staticmethod
+    def _modes(modes):
+        """Modes as the reference's params keys (intensity [W/cm^2], lambda [nm], ellipticity, cep,
+        delay, duration, envelope), converted as parameters.c:805-810."""
+        from ._lib import QND_ENV, LaserMode
+
+        arr = (LaserMode * max(1, len(modes)))()
+        for k, m in enumerate(modes):
+            if m["envelope"] not in QND_ENV:
+                raise ValueError(f"Unknown envelope: {m['envelope']}")
+            arr[k] = LaserMode(45.5637639947958 / m["lambda"], 5.33803e-9 * np.sqrt(m["intensity"]),
+                               m["ellipticity"], m["cep"], m["delay"], m["duration"], QND_ENV[m["envelope"]])
+        return arr
+
+    def field_samples(self, modes, nsteps):
+        """E, A [nsteps, s, dim] at the sub-step times and alpha [nsteps, dim] = A(i dt), computed on
+        the device (Initialize_field_vectors, integrators.c:74-101)."""
+        E = np.zeros((nsteps, self.s, self.dim))
+        A = np.zeros((nsteps, self.s, self.dim))
+        al = np.zeros((nsteps, self.dim))
+        check(lib().qnd_field_samples(self.h, len(modes), self._modes(modes), int(nsteps), E.ctypes.data,
+                                      A.ctypes.data, al.ctypes.data, 0))
+        return E, A, al
+
+    def field_samples_dev(self, modes, nsteps, E_dev=None, A_dev=None, alpha_dev=None):
+        """The same into device buffers (torch tensors or pointers), asynchronously on the stream."""
+        ptr = lambda x: None if x is None else _ptr_of(x)
+        check(lib().qnd_field_samples(self.h, len(modes), self._modes(modes), int(nsteps), ptr(E_dev), ptr(A_dev),
+                                      ptr(alpha_dev), 1))
+
+    def embed(self, psi, src, coeff=1.0, accumulate=False):
+        """psi <- (psi if accumulate else 0) + coeff * src centred on this grid (Read_wavefunction_MPI's
+        centring and superposition, io_functions.c:292-459); src is a host complex128 array."""
+        src = np.ascontiguousarray(src, dtype=np.complex128)
+        if src.ndim != self.dim:
+            raise ValueError("src needs DIMENSION axes")
+        nr = (C.c_int64 * self.dim)(*src.shape)
+        c = complex(coeff)
+        check(lib().qnd_state_embed(self.h, C.c_void_p(_ptr_of(psi)), src.ctypes.data_as(C.POINTER(C.c_double)), nr,
+                                    c.real, c.imag, int(bool(accumulate))))
