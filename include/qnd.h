@@ -160,6 +160,18 @@ int qnd_final_spectra(qnd_ctx *ctx, const void *psi_r_dev, double r_mask_min, do
 int qnd_observables_rspace_noalloc(qnd_ctx *ctx, const void *psi_r_dev, int nobs, const char *const *names,
                                    double *out_dev);
 
+/* ---- adjoint gradient of a length-gauge run (no reference counterpart: the differentiation
+ *      extension). From psi0_dev (r-space, not modified) it runs nsteps length-gauge steps with the
+ *      field samples E_host [nsteps][s][dim] (the step mask applies as in qnd_run_length), evaluates
+ *      J = dNr sum_x w(x) |psi_T(x)|^2 for the real weight w_host[n] (natural order; e.g. 1 beyond
+ *      |r| > R: the norm absorbed there), and writes dJ/dE[k][ia][j] for every sample into
+ *      grad_host [nsteps][s][dim], by running the adjoint state backward through the steps.
+ *      The forward states are kept every `checkpoint` steps and recomputed in between: the device
+ *      holds ceil(nsteps/checkpoint) + checkpoint + s + 2 states. J_out and psiT_dev (psi(T)) may be
+ *      NULL. Synchronises. */
+int qnd_adjoint_length(qnd_ctx *ctx, const void *psi0_dev, const double *E_host, int64_t nsteps, const double *w_host,
+                       int64_t checkpoint, double *J_out, double *grad_host, void *psiT_dev);
+
 /* ---- laser field on the device: replaces Initialize_field_vectors (integrators.c:74-101) and
  *      Field_vectors (parameters.c:899-949).
  * One mode of the field, as the reference holds it after parameters.c:805-810: frequency

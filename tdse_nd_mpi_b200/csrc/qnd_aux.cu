@@ -415,6 +415,23 @@ __global__ void __launch_bounds__(256) add_potential_kernel(long long n, cplx_t<
         dst[i] = cadd(dst[i], cscale(src[i], R(vtab[i])));
 }
 
+struct MaskArgs {
+    int dim;
+    int shift[MAX_DIM];
+    long long nmask[MAX_DIM];
+    const void* mask[MAX_DIM];
+};
+
+template <typename R>
+__global__ void __launch_bounds__(256) apply_masks_kernel(long long n, cplx_t<R>* psi, const __grid_constant__ MaskArgs a) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        cplx_t<R> x = psi[i];
+        for (int j = 0; j < a.dim; ++j)
+            if (a.mask[j]) x = cscale(x, static_cast<const R*>(a.mask[j])[(i >> a.shift[j]) & a.nmask[j]]);
+        psi[i] = x;
+    }
+}
+
 static int elementwise_blocks(long long n) {
     long long nb = (n + 255) / 256;
     if (nb > 148 * 16) nb = 148 * 16;
@@ -432,6 +449,17 @@ template <typename R> void launch_point_factors(long long n, cplx_t<R>* psi, con
                                                 const cplx_t<R>* pc, const R* pr, const double* scale_dev,
                                                 cudaStream_t st) {
     point_factors_kernel<R><<<elementwise_blocks(n), 256, 0, st>>>(n, psi, tr, tc, pc, pr, scale_dev);
+}
+template <typename R> void launch_apply_masks(long long n, cplx_t<R>* psi, int dim, const int* shift,
+                                              const long long* nmask, const R* const* masks, cudaStream_t st) {
+    MaskArgs a{};
+    a.dim = dim;
+    for (int j = 0; j < dim; ++j) {
+        a.shift[j] = shift[j];
+        a.nmask[j] = nmask[j];
+        a.mask[j] = masks[j];
+    }
+    apply_masks_kernel<R><<<elementwise_blocks(n), 256, 0, st>>>(n, psi, a);
 }
 template <typename R> void launch_add_potential(long long n, cplx_t<R>* dst, const cplx_t<R>* src, const double* vtab,
                                                 cudaStream_t st) {
@@ -453,7 +481,9 @@ template <typename R> void launch_add_potential(long long n, cplx_t<R>* dst, con
     template void launch_point_factors<R>(long long, cplx_t<R>*, const R*, const cplx_t<R>*, const cplx_t<R>*, \
                                           const R*, const double*, cudaStream_t);                          \
     template void launch_add_potential<R>(long long, cplx_t<R>*, const cplx_t<R>*, const double*, cudaStream_t); \
-    template void launch_embed<R>(const EmbedArgs&, const double2*, cplx_t<R>*, cudaStream_t);
+    template void launch_embed<R>(const EmbedArgs&, const double2*, cplx_t<R>*, cudaStream_t);                \
+    template void launch_apply_masks<R>(long long, cplx_t<R>*, int, const int*, const long long*, const R* const*, \
+                                        cudaStream_t);
 QND_INST(double)
 QND_INST(float)
 #undef QND_INST

@@ -350,7 +350,7 @@ static const void* spec_table(qnd_ctx* c, int kind, int ax, double coef) {
     return ptr;
 }
 
-enum RtabKind { RT_IMAG = 0, RT_LENGTH = 1, RT_VEL = 2 };
+enum RtabKind { RT_IMAG = 0, RT_LENGTH = 1, RT_VEL = 2, RT_LENGTH_ADJ = 3 };
 static const double NO_COEF = 1e300;  // marks "no second factor"
 
 static inline double clamped_exp(double arg) { return std::exp(arg > MAX_EXP_ARG ? MAX_EXP_ARG : arg); }
@@ -359,6 +359,7 @@ static inline double clamped_exp(double arg) { return std::exp(arg > MAX_EXP_ARG
 //   RT_IMAG   (a[, b]):  exp(min(700, -a V)) [* exp(min(700, -b V))]           real (integrators.c:143-160)
 //   RT_LENGTH (h):       exp(min(700, -h Vcap)) exp(-i h V)                      complex (integrators.c:186-188)
 //   RT_VEL    (a[, b]):  exp(min(700,-a Vcap)) exp(-i a V) [* same with b]       complex (integrators.c:209-229)
+//   RT_LENGTH_ADJ (h):   the complex conjugate of RT_LENGTH (the adjoint of that factor)
 // Reorder a full-grid array (comps values per point) to line-major order for axis ax: entry
 // lam*L + m holds point m of line lam (the order in which a pass along ax visits the grid).
 static std::vector<double> line_major(const qnd_ctx* c, const std::vector<double>& nat, int comps, int ax) {
@@ -412,7 +413,7 @@ static const void* rtab(qnd_ctx* c, int kind, double a, double b, int ax) {
             const double vc = c->vcap.empty() ? 0.0 : c->vcap[i];
             double re, im;
             if (c->fp64) {
-                if (kind == RT_LENGTH) {
+                if (kind == RT_LENGTH || kind == RT_LENGTH_ADJ) {
                     const double m = clamped_exp(-a * vc), th = a * c->vpot[i];
                     re = m * std::cos(th);
                     im = -m * std::sin(th);
@@ -443,7 +444,7 @@ static const void* rtab(qnd_ctx* c, int kind, double a, double b, int ax) {
                 im = di;
             }
             v[2 * i] = re;
-            v[2 * i + 1] = im;
+            v[2 * i + 1] = kind == RT_LENGTH_ADJ ? -im : im;  // conj(w), and for FP32 conj(w - 1) = conj(w) - 1
         }
         upload_cplx(c, *buf, line_major(c, v, 2, ax));
     }
@@ -1122,7 +1123,10 @@ static void run_chain(qnd_ctx* c, void* psi, const std::vector<ChainK>& K, const
         return;
     }
     auto finish = [&](PassSpec& ps) {
-        set_factor(c, post.f, ps.axis, post.lst, &ps.epi_real, &ps.epi_cplx, nullptr);
+        // laser phases after the chain go in the last pass's epilogue (its prologue must have none)
+        const bool lasers = post.f.laser_ia >= 0;
+        if (lasers && ps.ax_in_prologue) QND_FAIL(QND_EINVAL, "internal: laser phases on both sides of one pass");
+        set_factor(c, post.f, ps.axis, post.lst, &ps.epi_real, &ps.epi_cplx, lasers ? ps.ax_cplx : nullptr);
         if (post.mask)
             for (int j = 0; j < d; ++j) ps.ax_real[j] = c->mask_dev[j].p;
         if (post.red) ps.red = *post.red;
@@ -1489,6 +1493,166 @@ static void run_realtime(qnd_ctx* c, void* psi, const double* field_host, const 
         }
     }
     QND_CK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------- adjoint --
+//
+// Gradient of J = dNr sum_x w(x) |psi_T(x)|^2 with respect to every field sample E[k][i][j] of a
+// length-gauge run (an extension: the reference has no adjoint). A step is the operator product
+//   psi <- M K(a_{2s-1}) D_{s-1} K(c_{s-1}) ... D_0 K(c_0) psi,  c_0 = a_0, c_i = a_{2i-1} + a_{2i},
+// with the kinetic sandwiches K(c) (unitary), the step mask M (real, diagonal) and the potential
+// factors D_i = exp(-h_i Vcap) exp(-i h_i (V + x.E[k][i])), h_i = a_{2i} + a_{2i+1} (integrators.c:
+// 170-194 in r-space). With the adjoint state lambda = dJ/dconj(psi) (lambda_T = dNr w psi_T),
+// every operator O maps lambda <- O^dagger lambda going backward, and the factor D_i contributes
+//   dJ/dE[k][i][j] = 2 Re <lambda', -i h_i x_j psi'> = 2 h_i sum_x x_j Im(conj(lambda') psi'),
+// where psi' and lambda' are the state and the adjoint state just after D_i. O^dagger: K(-c) for
+// K(c), M for M, conj(D_i) = RT_LENGTH_ADJ times the laser phases of -E for D_i. The forward states
+// are kept every `every` steps; a segment's step-start states are recomputed from its checkpoint,
+// and a step's sub-step states from its start.
+
+// psi <- M psi for the step masks set on the axes.
+static void apply_step_masks(qnd_ctx* c, void* psi) {
+    if (c->fp64) {
+        const double* m[MAX_DIM] = {c->mask_dev[0].as<double>(), c->mask_dev[1].as<double>(), c->mask_dev[2].as<double>()};
+        long long nm[MAX_DIM];
+        for (int j = 0; j < MAX_DIM; ++j) nm[j] = c->nr[j] - 1;
+        launch_apply_masks<double>(c->n, static_cast<double2*>(psi), c->dim, c->shift, nm, m, c->stream);
+    } else {
+        const float* m[MAX_DIM] = {c->mask_dev[0].as<float>(), c->mask_dev[1].as<float>(), c->mask_dev[2].as<float>()};
+        long long nm[MAX_DIM];
+        for (int j = 0; j < MAX_DIM; ++j) nm[j] = c->nr[j] - 1;
+        launch_apply_masks<float>(c->n, static_cast<float2*>(psi), c->dim, c->shift, nm, m, c->stream);
+    }
+    c->kernels_launched++;
+    QND_CK(cudaGetLastError());
+}
+
+static void copy_state(qnd_ctx* c, void* dst, const void* src) {
+    QND_CK(cudaMemcpyAsync(dst, src, size_t(c->n) * c->elem(), cudaMemcpyDeviceToDevice, c->stream));
+}
+
+// Length-gauge steps k0 .. k0+n-1 of the run's field (host [nsteps][s][dim]) on an r-space psi.
+static void length_span(qnd_ctx* c, void* psi, const double* E, int64_t k0, int64_t n, bool masked) {
+    const int64_t chunk = chunk_steps(c);
+    for (int64_t q = 0; q < n; q += chunk) {
+        const int64_t ch = std::min(chunk, n - q);
+        upload_field_chunk(c, E + size_t(k0 + q) * c->s * c->dim, ch, false);
+        length_steps(c, psi, 0, ch, RedFn(), masked);
+    }
+}
+
+static void adjoint_length(qnd_ctx* c, const void* psi0, const double* E, int64_t nsteps, const double* w_host,
+                           int64_t every, double* J_out, double* grad_host, void* psiT) {
+    const int s = c->s, d = c->dim;
+    const size_t sb = size_t(c->n) * c->elem();
+    const int64_t K = std::max<int64_t>(1, std::min(every, nsteps));
+    const int64_t nck = (nsteps + K - 1) / K;
+    const bool masked = has_mask(c);
+    DevBuf ck, seg, sub, work, lam, wgrid, wscaled, out;
+    ck.ensure(size_t(nck) * sb);
+    seg.ensure(size_t(K) * sb);
+    sub.ensure(size_t(s) * sb);
+    work.ensure(sb);
+    lam.ensure(sb);
+    out.ensure((size_t(nsteps) * s * d + 1) * sizeof(double));
+    auto at = [&](DevBuf& b, int64_t k) { return static_cast<void*>(static_cast<char*>(b.p) + size_t(k) * sb); };
+    // the weight: FP64 for J, and dNr w in the state's precision for lambda_T
+    std::vector<double> w(w_host, w_host + c->n), wl(size_t(c->n));
+    for (size_t i = 0; i < wl.size(); ++i) wl[i] = c->dNr * w[i];
+    upload_f64(c, wgrid, w);
+    upload_real(c, wscaled, wl);
+
+    // forward, keeping the checkpoints
+    copy_state(c, work.p, psi0);
+    for (int64_t q = 0; q < nck; ++q) {
+        copy_state(c, at(ck, q), work.p);
+        length_span(c, work.p, E, q * K, std::min(K, nsteps - q * K), masked);
+    }
+    if (psiT) copy_state(c, psiT, work.p);
+    double* grad_dev = out.as<double>();
+    double* J_dev = grad_dev + size_t(nsteps) * s * d;
+    RedDesc rj{};
+    rj.n = 1;
+    rj.kind[0] = RK_ABS2;
+    rj.wkind[0] = WK_GRID;
+    rj.wtab[0] = wgrid.as<double>();
+    rj.scale[0] = c->dNr;
+    rj.out = J_dev;
+    grid_reduce(c, work.p, rj);
+    copy_state(c, lam.p, work.p);
+    if (c->fp64)
+        launch_point_factors<double>(c->n, lam.as<double2>(), wscaled.as<double>(), nullptr, nullptr, nullptr, nullptr,
+                                     c->stream);
+    else
+        launch_point_factors<float>(c->n, lam.as<float2>(), wscaled.as<float>(), nullptr, nullptr, nullptr, nullptr,
+                                    c->stream);
+    c->kernels_launched++;
+
+    auto kin = [&](double coef) {
+        ChainK k;
+        k.kind = SP_LENGTH;
+        k.coef = coef;
+        return std::vector<ChainK>{k};
+    };
+    auto cst = [&](int i) { return i == 0 ? c->as[0] : c->as[2 * i - 1] + c->as[2 * i]; };
+    auto hst = [&](int i) { return c->as[2 * i] + c->as[2 * i + 1]; };
+    std::vector<double> fe(size_t(2) * s * d);
+    // backward, segment by segment
+    for (int64_t q = nck - 1; q >= 0; --q) {
+        const int64_t k0 = q * K, kn = std::min(K, nsteps - k0);
+        copy_state(c, work.p, at(ck, q));
+        for (int64_t k = 0; k < kn; ++k) {
+            copy_state(c, at(seg, k), work.p);
+            if (k + 1 < kn) length_span(c, work.p, E, k0 + k, 1, masked);
+        }
+        for (int64_t k = kn - 1; k >= 0; --k) {
+            const int64_t kk = k0 + k;
+            // field tables of this step: slot 0 the samples (forward), slot 1 their negatives (adjoint)
+            for (int q2 = 0; q2 < s * d; ++q2) {
+                fe[q2] = E[size_t(kk) * s * d + q2];
+                fe[s * d + q2] = -fe[q2];
+            }
+            upload_field_chunk(c, fe.data(), 2, false);
+            // the states just after each D_i
+            copy_state(c, work.p, at(seg, k));
+            for (int i = 0; i < s; ++i) {
+                ChainMid post;
+                post.f.kind = RT_LENGTH;
+                post.f.a = hst(i);
+                post.f.laser_ia = i;
+                post.lst = 0;
+                run_chain(c, work.p, kin(cst(i)), {}, Factor{}, 0, nullptr, post);
+                copy_state(c, at(sub, i), work.p);
+            }
+            // lambda back through M and K(a_{2s-1})
+            if (masked) apply_step_masks(c, lam.p);
+            run_chain(c, lam.p, kin(-c->as[2 * s - 1]), {}, Factor{}, 0, nullptr, ChainMid{});
+            for (int i = s - 1; i >= 0; --i) {
+                RedDesc rg{};
+                rg.n = d;
+                for (int j = 0; j < d; ++j) {
+                    rg.kind[j] = RK_BILIN_IM;
+                    rg.wkind[j] = WK_AXIS;
+                    rg.waxis[j] = j;
+                    rg.wtab[j] = c->r_dev.as<double>() + c->axoff[j];
+                    rg.scale[j] = 2.0 * hst(i);
+                }
+                rg.out = grad_dev + (size_t(kk) * s + i) * d;
+                grid_reduce(c, at(sub, i), rg, lam.p);
+                Factor adj;
+                adj.kind = RT_LENGTH_ADJ;
+                adj.a = hst(i);
+                adj.laser_ia = i;
+                run_chain(c, lam.p, kin(-cst(i)), {}, adj, 1, nullptr, ChainMid{});
+            }
+        }
+    }
+    QND_CK(cudaMemcpyAsync(grad_host, grad_dev, size_t(nsteps) * s * d * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream));
+    double J = 0.0;
+    QND_CK(cudaMemcpyAsync(&J, J_dev, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    QND_CK(cudaStreamSynchronize(c->stream));
+    if (J_out) *J_out = J;
 }
 
 // ---------------------------------------------------------------- Gram-Schmidt --
@@ -2333,6 +2497,22 @@ int qnd_final_spectra(qnd_ctx* ctx, const void* psi_r_dev, double r_mask_min, do
                                ctx->stream));
         QND_CK(cudaStreamSynchronize(ctx->stream));
     }
+    QND_API_END
+}
+
+int qnd_adjoint_length(qnd_ctx* ctx, const void* psi0_dev, const double* E_host, int64_t nsteps, const double* w_host,
+                       int64_t checkpoint, double* J_out, double* grad_host, void* psiT_dev) {
+    using namespace qnd;
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi0_dev);
+    QND_NEED(w_host);
+    if (nsteps < 1) QND_FAIL(QND_EINVAL, "qnd_adjoint_length: nsteps %lld < 1", (long long)nsteps);
+    QND_NEED(E_host);
+    QND_NEED(grad_host);
+    if (checkpoint < 1) QND_FAIL(QND_EINVAL, "qnd_adjoint_length: checkpoint interval %lld < 1", (long long)checkpoint);
+    set_device(ctx);
+    adjoint_length(ctx, psi0_dev, E_host, nsteps, w_host, checkpoint, J_out, grad_host, psiT_dev);
     QND_API_END
 }
 

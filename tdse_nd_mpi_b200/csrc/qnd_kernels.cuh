@@ -146,6 +146,9 @@ template <typename R> void launch_long_transpose(const LongArgs& a, const cplx_t
 template <typename R> void launch_point_factors(long long n, cplx_t<R>* psi, const R* tr, const cplx_t<R>* tc,
                                                 const cplx_t<R>* pc, const R* pr, const double* scale_dev,
                                                 cudaStream_t st);
+// psi *= prod_j mask_j[index along axis j] over the axes whose mask is set (natural layout)
+template <typename R> void launch_apply_masks(long long n, cplx_t<R>* psi, int dim, const int* shift,
+                                              const long long* nmask, const R* const* masks, cudaStream_t st);
 // dst += vtab * src (H psi = T psi + V psi)
 template <typename R> void launch_add_potential(long long n, cplx_t<R>* dst, const cplx_t<R>* src, const double* vtab,
                                                 cudaStream_t st);

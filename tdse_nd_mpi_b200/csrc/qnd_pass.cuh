@@ -36,7 +36,8 @@ constexpr int MAX_RED = 8;
 constexpr int MAX_DIM = 3;
 
 enum : int { PM_SANDWICH = 0, PM_FFT_FWD = 1, PM_FFT_INV = 2, PM_SPECRED = 3, PM_APPLY = 4, PM_DOUBLE = 5, PM_NMODES = 6 };
-enum : int { RK_ABS2 = 0, RK_BILIN = 1 };          // |v|^2 * w   or   Re(conj(partner) * v) * w
+// |v|^2 w, Re(conj(partner) v) w, or (element-wise grid reductions only) Im(conj(partner) v) w
+enum : int { RK_ABS2 = 0, RK_BILIN = 1, RK_BILIN_IM = 2 };
 enum : int { WK_ONE = 0, WK_AXIS = 1, WK_GRID = 2 }; // weight 1, table[idx_axis], line-major table
 
 struct RedDesc {
@@ -162,9 +163,12 @@ __device__ __forceinline__ void accumulate_red(const RedDesc& rd, double* acc, V
         double val;
         if (rd.kind[k] == RK_ABS2) {
             val = double(v.x) * double(v.x) + double(v.y) * double(v.y);
-        } else {
+        } else if (rd.kind[k] == RK_BILIN) {
             V p = partner[flat];
             val = double(p.x) * double(v.x) + double(p.y) * double(v.y);
+        } else {
+            V p = partner[flat];
+            val = double(p.x) * double(v.y) - double(p.y) * double(v.x);
         }
         const int wk = rd.wkind[k];
         if (wk == WK_AXIS) {
