@@ -160,6 +160,17 @@ int qnd_final_spectra(qnd_ctx *ctx, const void *psi_r_dev, double r_mask_min, do
 int qnd_observables_rspace_noalloc(qnd_ctx *ctx, const void *psi_r_dev, int nobs, const char *const *names,
                                    double *out_dev);
 
+/* ---- a sweep of independent members in one graph (no reference counterpart: the reference runs
+ *      one propagation per job). Member i is qnd_run_length_dev(ctxs[i], psi_r_dev[i], E_dev[i],
+ *      nsteps, nobs, names, obs_dev[i]) (same nsteps and observables; grids, integrators, precisions
+ *      and potentials may differ; every context on the same device, each once). Per chunk of steps
+ *      the members' chains are the parallel branches of one CUDA graph, captured once and replayed,
+ *      so the small grids' passes overlap on the GPU with one graph launch per chunk. Members whose
+ *      observables need more than the fused reductions run one after another instead. Returns
+ *      after the last chunk has run (synchronises). */
+int qnd_run_length_batch(int count, qnd_ctx *const *ctxs, void *const *psi_r_dev, const double *const *E_dev,
+                         int64_t nsteps, int nobs, const char *const *names, double *const *obs_dev);
+
 /* ---- adjoint gradient of a length-gauge run (no reference counterpart: the differentiation
  *      extension). From psi0_dev (r-space, not modified) it runs nsteps length-gauge steps with the
  *      field samples E_host [nsteps][s][dim] (the step mask applies as in qnd_run_length), evaluates

@@ -2,7 +2,9 @@
 (members), each its own real-time length-gauge run.
 
 - On one GPU every member has its own context and stream, so the small grids' passes overlap.
-  One 256^2 pass fills a tenth of a B200.
+  One 256^2 pass fills a tenth of a B200. By default the members' chains of each chunk of steps
+  are the parallel branches of one CUDA graph (qnd_run_length_batch): one graph launch per chunk
+  for the whole sweep.
 - Across ranks the members are shared out by a balanced-bytes greedy, with no data exchange during
   the runs. The observables are gathered on rank 0 at the end.
 """
@@ -50,10 +52,16 @@ def partition(members, world: int) -> list[list[int]]:
     return parts
 
 
-def run_members(members) -> list[dict]:
+def run_members(members, one_graph: bool = True) -> list[dict]:
     """Run the members on the current GPU, concurrently; returns per member the observable rows after
-    every step ([nsteps][nvalues], as qnd_run_length_dev) and the final state."""
+    every step ([nsteps][nvalues], as qnd_run_length_dev) and the final state. one_graph: all members
+    through qnd_run_length_batch (needs the same nsteps and observables); otherwise each member's own
+    device loop on its own stream."""
+    import ctypes as C
+
     import torch
+
+    from ._lib import check, lib
 
     runs = []
     for m in members:
@@ -69,8 +77,18 @@ def run_members(members) -> list[dict]:
         obs = torch.zeros((E.shape[0], max(nv, 1)), dtype=torch.float64, device="cuda")
         runs.append((g, st, E, obs, nv))
     torch.cuda.synchronize()  # inputs on the device before the contexts' own streams read them
-    for (g, st, E, obs, nv), m in zip(runs, members):
-        g.run_length_dev(st, E, E.shape[0], list(m.names), obs if nv else None)
+    same = len({(r[2].shape[0], tuple(m.names)) for r, m in zip(runs, members)}) == 1
+    if one_graph and same and runs:
+        k = len(runs)
+        names = list(members[0].names)
+        arr = lambda xs: (C.c_void_p * k)(*xs)
+        cnames = (C.c_char_p * max(1, len(names)))(*[n.encode() for n in names])
+        check(lib().qnd_run_length_batch(k, arr([r[0].h for r in runs]), arr([r[1].ptr for r in runs]),
+                                         arr([r[2].data_ptr() for r in runs]), int(runs[0][2].shape[0]), len(names),
+                                         cnames, arr([r[3].data_ptr() for r in runs])))
+    else:
+        for (g, st, E, obs, nv), m in zip(runs, members):
+            g.run_length_dev(st, E, E.shape[0], list(m.names), obs if nv else None)
     out = []
     for g, st, E, obs, nv in runs:
         g.synchronize()

@@ -1541,6 +1541,15 @@ static void length_span(qnd_ctx* c, void* psi, const double* E, int64_t k0, int6
     }
 }
 
+// One member of qnd_run_length_batch: its context, observables, mask and staged rows.
+struct SweepMember {
+    qnd_ctx* c = nullptr;
+    std::vector<ObsItem> items;
+    int nv = 0;
+    bool masked = false;
+    double* stage = nullptr;
+};
+
 static void adjoint_length(qnd_ctx* c, const void* psi0, const double* E, int64_t nsteps, const double* w_host,
                            int64_t every, double* J_out, double* grad_host, void* psiT) {
     const int s = c->s, d = c->dim;
@@ -2497,6 +2506,158 @@ int qnd_final_spectra(qnd_ctx* ctx, const void* psi_r_dev, double r_mask_min, do
                                ctx->stream));
         QND_CK(cudaStreamSynchronize(ctx->stream));
     }
+    QND_API_END
+}
+
+int qnd_run_length_batch(int count, qnd_ctx* const* ctxs, void* const* psi_r_dev, const double* const* E_dev,
+                         int64_t nsteps, int nobs, const char* const* names, double* const* obs_dev) {
+    using namespace qnd;
+    QND_API_BEGIN
+    if (count < 1) QND_FAIL(QND_EINVAL, "qnd_run_length_batch: count %d < 1", count);
+    QND_NEED(ctxs);
+    QND_NEED(psi_r_dev);
+    QND_NEED(E_dev);
+    if (nobs > 0) QND_NEED(names);
+    for (int i = 0; i < count; ++i) {
+        QND_NEED(ctxs[i]);
+        QND_NEED(psi_r_dev[i]);
+        QND_NEED(E_dev[i]);
+        if (ctxs[i]->device != ctxs[0]->device) QND_FAIL(QND_EINVAL, "qnd_run_length_batch: members on different devices");
+        for (int j = 0; j < i; ++j)
+            if (ctxs[j] == ctxs[i]) QND_FAIL(QND_EINVAL, "qnd_run_length_batch: a context appears twice");
+    }
+    if (nsteps <= 0) return QND_OK;
+    set_device(ctxs[0]);
+    std::vector<SweepMember> ms(static_cast<size_t>(count));
+    bool one_graph = true;
+    int64_t chunk = CHUNK;
+    for (int i = 0; i < count; ++i) {
+        SweepMember& m = ms[i];
+        m.c = ctxs[i];
+        m.items = parse_obs(m.c, nobs, names, &m.nv);
+        if (m.nv > 0) QND_NEED(obs_dev);
+        if (m.nv > 0 && obs_dev) QND_NEED(obs_dev[i]);
+        m.masked = has_mask(m.c);
+        std::vector<double> probe(size_t(m.nv) + 1);  // only the descriptor count is wanted here
+        if (m.nv > 0 && !(all_rspace(m.items) && rspace_red(m.c, m.items, probe.data(), 0).size() <= 1))
+            one_graph = false;
+        chunk = std::min(chunk, chunk_steps(m.c));
+    }
+    if (!one_graph) {
+        // observables beyond one fused descriptor: each member's own device loop
+        for (int i = 0; i < count; ++i) {
+            const int rc = qnd_run_length_dev(ctxs[i], psi_r_dev[i], E_dev[i], nsteps, nobs, names,
+                                              ms[i].nv ? obs_dev[i] : nullptr);
+            if (rc != QND_OK) return rc;
+        }
+        return QND_OK;
+    }
+    for (SweepMember& m : ms)
+        if (m.nv > 0) {
+            m.c->obs_dev.ensure(size_t(chunk) * m.nv * sizeof(double));
+            m.stage = m.c->obs_dev.as<double>();
+        }
+    // a root stream forks to every member's stream and joins them again: the members' chains of one
+    // chunk are the parallel branches of one graph
+    struct Res {
+        cudaStream_t root = nullptr;
+        cudaEvent_t fork = nullptr;
+        std::vector<cudaEvent_t> join;
+        cudaGraphExec_t exec = nullptr;
+        ~Res() {
+            if (root) cudaStreamSynchronize(root);
+            if (exec) cudaGraphExecDestroy(exec);
+            if (fork) cudaEventDestroy(fork);
+            for (cudaEvent_t e : join)
+                if (e) cudaEventDestroy(e);
+            if (root) cudaStreamDestroy(root);
+        }
+    } r;
+    QND_CK(cudaStreamCreateWithFlags(&r.root, cudaStreamNonBlocking));
+    QND_CK(cudaEventCreateWithFlags(&r.fork, cudaEventDisableTiming));
+    r.join.assign(size_t(count), nullptr);
+    for (auto& e : r.join) QND_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    auto fork_members = [&]() {
+        QND_CK(cudaEventRecord(r.fork, r.root));
+        for (SweepMember& m : ms) QND_CK(cudaStreamWaitEvent(m.c->stream, r.fork, 0));
+    };
+    auto join_members = [&]() {
+        for (int i = 0; i < count; ++i) {
+            QND_CK(cudaEventRecord(r.join[i], ms[i].c->stream));
+            QND_CK(cudaStreamWaitEvent(r.root, r.join[i], 0));
+        }
+    };
+    auto chains = [&](int64_t ch) {
+        for (SweepMember& m : ms) {
+            RedFn rf;
+            if (m.nv > 0) {
+                SweepMember* mp = &m;
+                rf = [mp](int64_t k, int ax) { return rspace_red(mp->c, mp->items, mp->stage + size_t(k) * mp->nv, ax); };
+            }
+            length_steps(m.c, psi_r_dev[&m - ms.data()], 0, ch, rf, m.masked);
+        }
+    };
+    std::string exec_key, warm_key;
+    std::vector<int64_t> launches(size_t(count), 0);  // per member, kernels in one replay of the graph
+    for (int64_t c0 = 0; c0 < nsteps; c0 += chunk) {
+        const int64_t ch = std::min(chunk, nsteps - c0);
+        for (int i = 0; i < count; ++i)
+            build_field_tables(ms[i].c, E_dev[i] + size_t(c0) * ms[i].c->s * ms[i].c->dim, ch, false);
+        join_members();  // the root waits for every member's tables (and its earlier work)
+        std::string key = fmt("%lld|", (long long)ch);
+        for (int i = 0; i < count; ++i)
+            key += chain_key(ms[i].c, psi_r_dev[i], ch, nobs, names, ms[i].stage, ms[i].masked) + "#";
+        if (r.exec && key == exec_key) {
+            QND_CK(cudaGraphLaunch(r.exec, r.root));
+            // the launch counters advance as for direct launches (they seed the FP32 dithering)
+            for (int i = 0; i < count; ++i) ms[i].c->kernels_launched += launches[i];
+        } else if (key != warm_key || std::getenv("QND_NO_GRAPH")) {
+            // first chunk of this shape: direct launches (they build the tables the chains read)
+            fork_members();
+            chains(ch);
+            join_members();
+            warm_key = key;
+        } else {
+            if (r.exec) {
+                QND_CK(cudaStreamSynchronize(r.root));
+                cudaGraphExecDestroy(r.exec);
+                r.exec = nullptr;
+            }
+            for (int i = 0; i < count; ++i) launches[i] = ms[i].c->kernels_launched;
+            QND_CK(cudaStreamBeginCapture(r.root, cudaStreamCaptureModeThreadLocal));
+            cudaGraph_t g = nullptr;
+            try {
+                fork_members();
+                chains(ch);
+                join_members();
+            } catch (...) {
+                cudaStreamEndCapture(r.root, &g);
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                throw;
+            }
+            QND_CK(cudaStreamEndCapture(r.root, &g));
+            for (int i = 0; i < count; ++i) launches[i] = ms[i].c->kernels_launched - launches[i];
+            const cudaError_t e = cudaGraphInstantiate(&r.exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                r.exec = nullptr;
+                QND_FAIL(QND_ECUDA, "cudaGraphInstantiate of a batch chunk: %s", cudaGetErrorString(e));
+            }
+            exec_key = key;
+            QND_CK(cudaGraphLaunch(r.exec, r.root));
+        }
+        // each member's rows of this chunk to the caller, after the chunk
+        fork_members();
+        for (int i = 0; i < count; ++i)
+            if (ms[i].nv > 0)
+                QND_CK(cudaMemcpyAsync(obs_dev[i] + size_t(c0) * ms[i].nv, ms[i].stage,
+                                       size_t(ch) * ms[i].nv * sizeof(double), cudaMemcpyDeviceToDevice,
+                                       ms[i].c->stream));
+    }
+    join_members();
+    QND_CK(cudaGetLastError());
     QND_API_END
 }
 

@@ -89,3 +89,33 @@ def test_concurrent_members_match_one_by_one(qnd_lib):
         np.testing.assert_array_equal(obs.cpu().numpy(), r["obs"])
         np.testing.assert_array_equal(st.download(), r["psi"])
         g.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_one_graph_sweep_matches_members_alone(qnd_lib, precision, monkeypatch):
+    """qnd_run_length_batch over uneven grids, Verlet and BM4 members, 1-D and 2-D, 434 steps
+    (chunks: direct, captured, replayed, a shorter direct one): every member's rows and final state
+    equal its own run_length_dev, bit for bit; and equal the batch run with the graph switched off."""
+    import dataclasses
+
+    from tdse_nd_mpi_b200.batch import run_members
+
+    def long_member(shape, seed, integ="BM4"):
+        m = _member(shape, seed, integ)
+        rng = np.random.default_rng(100 + seed)
+        s = 1 if integ == "Verlet" else 6
+        return dataclasses.replace(m, field=rng.standard_normal((434, s, len(shape))) * 0.05, precision=precision)
+
+    members = [long_member((64, 64), 11), long_member((128, 64), 12, "Verlet"), long_member((32, 32), 13),
+               long_member((2048,), 14, "Verlet")]
+    together = run_members(members, one_graph=True)
+    alone = run_members(members, one_graph=False)
+    for a, b in zip(together, alone):
+        np.testing.assert_array_equal(a["obs"], b["obs"])
+        np.testing.assert_array_equal(a["psi"], b["psi"])
+    monkeypatch.setenv("QND_NO_GRAPH", "1")
+    direct = run_members(members, one_graph=True)
+    for a, b in zip(together, direct):
+        np.testing.assert_array_equal(a["obs"], b["obs"])
+        np.testing.assert_array_equal(a["psi"], b["psi"])
