@@ -388,6 +388,54 @@ def timed_steps_single(torch, grid, psi_t, E_dev, obs_dev, names, i0, steps, flu
     return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
 
 
+def sweep_leg(torch, steps):
+    """The sweep configuration: 96 H_2D length-gauge members (32 x 256^2, 48 x 512^2, 16 x 1024^2,
+    DR 0.2), BM4 and Verlet alternating, mixed precision, each with a seeded CEP in [0, 2 pi) and an
+    intensity log-uniform in [5e13, 3e14] W/cm^2 of an 800 nm 4-cycle sin^2 pulse (field samples from
+    qnd_field_samples), norm + dipole every step. `steps` steps from the pulse's middle, timed with
+    CUDA events around whole-sweep calls, each after an untimed call of the same shape: one CUDA graph
+    per chunk for all members (qnd_run_length_batch) and, for comparison, one stream per member."""
+    from tdse_nd_mpi_b200 import Grid
+    from tdse_nd_mpi_b200.batch import Member, launch, prepare, release
+
+    rng = np.random.default_rng(2024)
+    tau = 4 * 2 * np.pi / (45.5637639947958 / 800.0)
+    total = int(tau / DT)
+    i0 = max(0, total // 2 - steps // 2)
+    members = []
+    for k, n in enumerate([256] * 32 + [512] * 48 + [1024] * 16):
+        integ = "BM4" if k % 2 == 0 else "Verlet"
+        mode = {"intensity": float(np.exp(rng.uniform(np.log(5e13), np.log(3e14)))), "lambda": 800.0,
+                "ellipticity": 0.0, "cep": float(rng.uniform(0.0, 2 * np.pi)), "delay": 0.0, "duration": tau,
+                "envelope": "cos2"}
+        g = Grid(2, (n, n), (DR, DR), integ, DT)
+        E = g.field_samples([mode], i0 + steps)[0][i0:]
+        g.close()
+        x = -0.5 * n * DR + np.arange(n) * DR
+        X, Y = np.meshgrid(x, x, indexing="ij")
+        psi = np.exp(-(X * X + Y * Y) / 2.0).astype(np.complex128)
+        psi /= np.sqrt(np.sum(np.abs(psi) ** 2) * DR * DR)
+        members.append(Member(shape=(n, n), dr=(DR, DR), integrator=integ, dt=DT, potential="H_2D", field=E,
+                              psi0=psi, cap=(0.05, 5.0), names=("norm", "dipole_r"), precision="mixed"))
+    runs = prepare(members)
+    points = sum(n * n for n in [256] * 32 + [512] * 48 + [1024] * 16)
+    out = {"members": len(members), "grid_points": points, "steps": steps, "precision": "mixed",
+           "what": "whole-sweep calls, CUDA events around each (the call returns when all members are done)"}
+    for label, one in (("one_graph", True), ("streams", False)):
+        launch(runs, one)  # warm-up: tables, the chunk graphs of this shape
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        launch(runs, one)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        out[label] = {"ms": ms, "member_steps_per_s": len(members) * steps / (ms / 1e3),
+                      "point_steps_per_s": points * steps / (ms / 1e3)}
+    release(runs)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -396,6 +444,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-extras", action="store_true", help="skip mixed / cuFFT / CPU legs")
     ap.add_argument("--imag-steps", type=int, default=100, help="imaginary-time steps for the initial state")
+    ap.add_argument("--sweep", type=int, default=0, metavar="STEPS",
+                    help="also time the 96-member sweep configuration for STEPS steps (key 'sweep')")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -496,6 +546,10 @@ def main():
     names_c = (C.c_char_p * len(OBS))(*[s.encode() for s in OBS])
     L = _lib.lib()
     dptr = lambda tns: C.cast(C.c_void_p(tns.data_ptr()), C.POINTER(C.c_double))  # noqa: E731
+    # warm-up: one untimed call of the same shape (the engine captures its chunk graphs on first use)
+    _lib.check(L.qnd_state_upload(grid.h, C.c_void_p(psi_dev_e2e.data_ptr()), dptr(psi_host)))
+    _lib.check(L.qnd_run_length(grid.h, C.c_void_p(psi_dev_e2e.data_ptr()), dptr(E_host), e2e_steps, len(OBS),
+                                names_c, dptr(obs_host)))
     flush.zero_()
     torch.cuda.synchronize()
     if dist:
@@ -516,7 +570,8 @@ def main():
     e2e = {"value": job_throughput(world, e2e_steps, e2e_ms), "unit": "steps/s",
            "h2d_bytes_per_step": (n * 16 + e2e_steps * grid.s * 2 * 8) / e2e_steps,
            "d2h_bytes_per_step": (n * 16 + e2e_steps * nv * 8) / e2e_steps,
-           "what": "qnd_state_upload + qnd_run_length (host E, host observable rows) + qnd_state_download",
+           "what": "qnd_state_upload + qnd_run_length (host E, host observable rows) + qnd_state_download, "
+                   "after one untimed call of the same shape",
            "host_ms": {"upload": 1e3 * (h1 - h0), "run_length": 1e3 * (h2 - h1), "download": 1e3 * (h3 - h2)}}
 
     extras = {}
@@ -566,6 +621,8 @@ def main():
         "clocks": clk.summary(),
     }
     line.update(extras)
+    if args.sweep > 0 and world == 1:
+        line["sweep"] = sweep_leg(torch, args.sweep)
     if rank == 0:
         print(json.dumps(line), flush=True)
     grid.close()

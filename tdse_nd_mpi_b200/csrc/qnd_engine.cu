@@ -21,7 +21,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <atomic>
 #include <map>
+#include <set>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -111,6 +113,16 @@ static const int64_t LONG_AXIS_MAX = int64_t(1) << 24;  // longest 1-D axis (fou
 
 using namespace qnd;
 
+namespace qnd {
+struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int64_t> launches;  // kernels one replay launches, per context it spans
+    uint64_t last_use = 0;
+};
+constexpr size_t MAX_GRAPHS = 8;
+static std::atomic<uint64_t> g_ctx_serial{0};
+}  // namespace qnd
+
 struct qnd_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -171,14 +183,16 @@ struct qnd_ctx {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pairs;
     std::vector<cudaEvent_t> event_pool;
 
-    // A chunk-wide sandwich chain captured in a CUDA graph and replayed for the later chunks of the
-    // same shape: what it captured (key), the executable graph, the kernels one replay launches,
-    // and the key of the last chain run directly (its tables exist). config_epoch bumps with every
-    // setter that changes what a chain reads.
-    std::string chain_key, chain_warm;
-    cudaGraphExec_t chain_exec = nullptr;
-    int64_t chain_launches = 0;
+    // Chunk-wide sandwich chains captured in CUDA graphs and replayed for the later chunks of the
+    // same shape (run_chunk_graph): the executable graphs by what they captured (key; at most
+    // MAX_GRAPHS, least recently used first out), and the keys already run directly once (their
+    // tables exist). config_epoch bumps with every setter that changes what a chain reads; serial
+    // tells this context from any earlier one at the same addresses.
+    std::map<std::string, GraphEntry> graphs;
+    std::set<std::string> warm_keys;
+    uint64_t graph_clock = 0;
     uint64_t config_epoch = 0;
+    uint64_t serial = 0;
 
     size_t elem() const { return fp64 ? 16 : 8; }
     size_t rsize() const { return fp64 ? 8 : 4; }
@@ -1358,11 +1372,47 @@ static int64_t chunk_steps(const qnd_ctx* c) {
     return std::max<int64_t>(1, std::min<int64_t>(CHUNK, fit));
 }
 
+// The context's graph for key, or null; a hit counts as a use.
+static GraphEntry* find_graph(qnd_ctx* c, const std::string& key) {
+    auto it = c->graphs.find(key);
+    if (it == c->graphs.end()) return nullptr;
+    it->second.last_use = ++c->graph_clock;
+    return &it->second;
+}
+
+// Keep an instantiated graph under key; past MAX_GRAPHS the least recently used one goes (after the
+// device is idle, so that no launch of it is in flight).
+static GraphEntry* keep_graph(qnd_ctx* c, const std::string& key, cudaGraphExec_t ex, std::vector<int64_t> launches) {
+    if (c->graphs.size() >= MAX_GRAPHS) {
+        auto lru = c->graphs.begin();
+        for (auto it = c->graphs.begin(); it != c->graphs.end(); ++it)
+            if (it->second.last_use < lru->second.last_use) lru = it;
+        QND_CK(cudaDeviceSynchronize());
+        cudaGraphExecDestroy(lru->second.exec);
+        c->graphs.erase(lru);
+    }
+    GraphEntry& e = c->graphs[key];
+    e.exec = ex;
+    e.launches = std::move(launches);
+    e.last_use = ++c->graph_clock;
+    return &e;
+}
+
+// First sight of key: run directly and remember it; true if it had been seen before.
+static bool seen_before(qnd_ctx* c, const std::string& key) {
+    if (c->warm_keys.count(key)) return true;
+    if (c->warm_keys.size() >= 64) c->warm_keys.clear();
+    c->warm_keys.insert(key);
+    return false;
+}
+
 // Run a chunk-wide chain (body) through a CUDA graph. The first run of a key goes directly (it
 // builds the tables the chain reads); the second captures it; later runs replay the graph, so the
 // host enqueues one graph launch per chunk instead of ~7 kernels per step and the device does not
-// wait on a slow host. Direct runs when profiling (per-launch events), when the caller is already
-// capturing the stream, or with QND_NO_GRAPH set.
+// wait on a slow host. The graphs stay with the context (a few keys: a run's full and last chunks,
+// repeated calls), so a later call of the same shape replays from its first chunk. Direct runs
+// when profiling (per-launch events), when the caller is already capturing the stream, or with
+// QND_NO_GRAPH set.
 static void run_chunk_graph(qnd_ctx* c, const std::string& key, const std::function<void()>& body) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     QND_CK(cudaStreamIsCapturing(c->stream, &cs));
@@ -1370,20 +1420,14 @@ static void run_chunk_graph(qnd_ctx* c, const std::string& key, const std::funct
         body();
         return;
     }
-    if (c->chain_exec && c->chain_key == key) {
-        QND_CK(cudaGraphLaunch(c->chain_exec, c->stream));
-        c->kernels_launched += c->chain_launches;
+    if (GraphEntry* ge = find_graph(c, key)) {
+        QND_CK(cudaGraphLaunch(ge->exec, c->stream));
+        c->kernels_launched += ge->launches[0];
         return;
     }
-    if (c->chain_warm != key) {
+    if (!seen_before(c, key)) {
         body();
-        c->chain_warm = key;
         return;
-    }
-    if (c->chain_exec) {
-        cudaGraphExecDestroy(c->chain_exec);
-        c->chain_exec = nullptr;
-        c->chain_key.clear();
     }
     const int64_t k0 = c->kernels_launched;
     QND_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -1405,18 +1449,16 @@ static void run_chunk_graph(qnd_ctx* c, const std::string& key, const std::funct
         cudaGetLastError();
         QND_FAIL(QND_ECUDA, "cudaGraphInstantiate of a step chain: %s", cudaGetErrorString(e));
     }
-    c->chain_exec = ex;
-    c->chain_key = key;
-    c->chain_launches = c->kernels_launched - k0;
+    keep_graph(c, key, ex, {c->kernels_launched - k0});
     QND_CK(cudaGraphLaunch(ex, c->stream));
 }
 
 // What a length-gauge chunk chain captures (see run_chunk_graph).
 static std::string chain_key(qnd_ctx* c, const void* psi, int64_t ch, int nobs, const char* const* names,
                              const double* rows, bool masked) {
-    std::string k = fmt("L|%p|%lld|%p|%d|%p|%p|%p|%llu|%llu|%d|", psi, (long long)ch, (const void*)rows, int(masked),
-                        c->field_tab.p, c->partials.p, c->counter.p, (unsigned long long)c->table_epoch,
-                        (unsigned long long)c->config_epoch, int(c->pdl));
+    std::string k = fmt("L|%llu|%p|%lld|%p|%d|%p|%p|%p|%llu|%llu|%d|", (unsigned long long)c->serial, psi,
+                        (long long)ch, (const void*)rows, int(masked), c->field_tab.p, c->partials.p, c->counter.p,
+                        (unsigned long long)c->table_epoch, (unsigned long long)c->config_epoch, int(c->pdl));
     for (int q = 0; q < nobs; ++q) {
         k += names[q] ? names[q] : "";
         k += ',';
@@ -1909,6 +1951,7 @@ int qnd_ctx_create(int dim, const int64_t* nr, const double* dr, const char* int
     QND_NEED(dr);
     *out = nullptr;
     auto c = std::make_unique<qnd_ctx>();
+    c->serial = ++g_ctx_serial;
     build_context(c.get(), dim, nr, dr, integrator, dt, precision);
     *out = c.release();
     QND_API_END
@@ -1924,7 +1967,7 @@ int qnd_ctx_destroy(qnd_ctx* ctx) {
         cudaEventDestroy(pr.second);
     }
     for (auto e : ctx->event_pool) cudaEventDestroy(e);
-    if (ctx->chain_exec) cudaGraphExecDestroy(ctx->chain_exec);
+    for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second.exec);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     QND_API_END
@@ -2563,10 +2606,8 @@ int qnd_run_length_batch(int count, qnd_ctx* const* ctxs, void* const* psi_r_dev
         cudaStream_t root = nullptr;
         cudaEvent_t fork = nullptr;
         std::vector<cudaEvent_t> join;
-        cudaGraphExec_t exec = nullptr;
         ~Res() {
             if (root) cudaStreamSynchronize(root);
-            if (exec) cudaGraphExecDestroy(exec);
             if (fork) cudaEventDestroy(fork);
             for (cudaEvent_t e : join)
                 if (e) cudaEventDestroy(e);
@@ -2597,32 +2638,29 @@ int qnd_run_length_batch(int count, qnd_ctx* const* ctxs, void* const* psi_r_dev
             length_steps(m.c, psi_r_dev[&m - ms.data()], 0, ch, rf, m.masked);
         }
     };
-    std::string exec_key, warm_key;
-    std::vector<int64_t> launches(size_t(count), 0);  // per member, kernels in one replay of the graph
+    // the sweep's graphs live in the first member's context, keyed by every member's chain
+    qnd_ctx* home = ms[0].c;
+    const bool no_graph = std::getenv("QND_NO_GRAPH") != nullptr;
     for (int64_t c0 = 0; c0 < nsteps; c0 += chunk) {
         const int64_t ch = std::min(chunk, nsteps - c0);
         for (int i = 0; i < count; ++i)
             build_field_tables(ms[i].c, E_dev[i] + size_t(c0) * ms[i].c->s * ms[i].c->dim, ch, false);
         join_members();  // the root waits for every member's tables (and its earlier work)
-        std::string key = fmt("%lld|", (long long)ch);
+        std::string key = fmt("B%d|%lld|", count, (long long)ch);
         for (int i = 0; i < count; ++i)
             key += chain_key(ms[i].c, psi_r_dev[i], ch, nobs, names, ms[i].stage, ms[i].masked) + "#";
-        if (r.exec && key == exec_key) {
-            QND_CK(cudaGraphLaunch(r.exec, r.root));
+        GraphEntry* ge = no_graph ? nullptr : find_graph(home, key);
+        if (ge) {
+            QND_CK(cudaGraphLaunch(ge->exec, r.root));
             // the launch counters advance as for direct launches (they seed the FP32 dithering)
-            for (int i = 0; i < count; ++i) ms[i].c->kernels_launched += launches[i];
-        } else if (key != warm_key || std::getenv("QND_NO_GRAPH")) {
+            for (int i = 0; i < count; ++i) ms[i].c->kernels_launched += ge->launches[i];
+        } else if (no_graph || !seen_before(home, key)) {
             // first chunk of this shape: direct launches (they build the tables the chains read)
             fork_members();
             chains(ch);
             join_members();
-            warm_key = key;
         } else {
-            if (r.exec) {
-                QND_CK(cudaStreamSynchronize(r.root));
-                cudaGraphExecDestroy(r.exec);
-                r.exec = nullptr;
-            }
+            std::vector<int64_t> launches(static_cast<size_t>(count));
             for (int i = 0; i < count; ++i) launches[i] = ms[i].c->kernels_launched;
             QND_CK(cudaStreamBeginCapture(r.root, cudaStreamCaptureModeThreadLocal));
             cudaGraph_t g = nullptr;
@@ -2638,15 +2676,15 @@ int qnd_run_length_batch(int count, qnd_ctx* const* ctxs, void* const* psi_r_dev
             }
             QND_CK(cudaStreamEndCapture(r.root, &g));
             for (int i = 0; i < count; ++i) launches[i] = ms[i].c->kernels_launched - launches[i];
-            const cudaError_t e = cudaGraphInstantiate(&r.exec, g, 0);
+            cudaGraphExec_t ex = nullptr;
+            const cudaError_t e = cudaGraphInstantiate(&ex, g, 0);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) {
                 cudaGetLastError();
-                r.exec = nullptr;
                 QND_FAIL(QND_ECUDA, "cudaGraphInstantiate of a batch chunk: %s", cudaGetErrorString(e));
             }
-            exec_key = key;
-            QND_CK(cudaGraphLaunch(r.exec, r.root));
+            keep_graph(home, key, ex, std::move(launches));
+            QND_CK(cudaGraphLaunch(ex, r.root));
         }
         // each member's rows of this chunk to the caller, after the chunk
         fork_members();
