@@ -2317,12 +2317,26 @@ int qnd_imag_propagate(qnd_ctx* ctx, void* const* states_dev, int j, int64_t nst
     for (int k = 0; k <= j; ++k) QND_NEED(states_dev[k]);
     if (nsteps <= 0) return QND_OK;
     set_device(ctx);
-    const double* pending = nullptr;
-    for (int64_t st = 0; st < nsteps; ++st) {
-        imag_steps(ctx, states_dev[j], 1, pending);
-        gs_project(ctx, states_dev, j);
-        pending = ctx->scal.as<double>() + 1;
-        if ((st & 255) == 255) check_gs_flag(ctx, j);
+    // the first step, then blocks of up to CHUNK steps {step with the deferred normalisation,
+    // Gram-Schmidt}, each replayed from a CUDA graph once its shape has been seen (run_chunk_graph);
+    // the norm-collapse flag is read after every block
+    imag_steps(ctx, states_dev[j], 1, nullptr);
+    gs_project(ctx, states_dev, j);
+    const double* pending = ctx->scal.as<double>() + 1;
+    for (int64_t st = 1; st < nsteps; st += CHUNK) {
+        const int64_t n = std::min(CHUNK, nsteps - st);
+        std::string key = fmt("I|%llu|%d|%lld|%p|%p|%p|%p|%llu|%llu|%d|", (unsigned long long)ctx->serial, j,
+                              (long long)n, ctx->scal.p, ctx->gs_flag.p, ctx->partials.p, ctx->counter.p,
+                              (unsigned long long)ctx->table_epoch, (unsigned long long)ctx->config_epoch,
+                              int(ctx->pdl));
+        for (int k = 0; k <= j; ++k) key += fmt("%p,", states_dev[k]);
+        run_chunk_graph(ctx, key, [&]() {
+            for (int64_t q = 0; q < n; ++q) {
+                imag_steps(ctx, states_dev[j], 1, pending);
+                gs_project(ctx, states_dev, j);
+            }
+        });
+        check_gs_flag(ctx, j);
     }
     scale_state(ctx, states_dev[j], pending);
     check_gs_flag(ctx, j);
