@@ -77,6 +77,11 @@ struct DevBuf {
         if (p) cudaFree(p);
         p = nullptr;
         bytes = 0;
+        // fault injection for the tests: QND_FAIL_ALLOC_ABOVE=<bytes> makes every larger request fail
+        // here, on the host, as an out-of-memory would
+        if (const char* lim = std::getenv("QND_FAIL_ALLOC_ABOVE"))
+            if (b > size_t(std::strtoull(lim, nullptr, 10)))
+                QND_FAIL(QND_ENOMEM, "cudaMalloc(%zu bytes): refused by QND_FAIL_ALLOC_ABOVE=%s", b, lim);
         cudaError_t e = cudaMalloc(&p, b ? b : 16);
         if (e != cudaSuccess) {
             cudaGetLastError();

@@ -1,0 +1,65 @@
+"""Failure paths, with every fault made on the host (no GPU fault, trap or hang):
+
+* a device allocation refused through the QND_FAIL_ALLOC_ABOVE hook: a QND_ENOMEM status with the
+  request's size, and the context works again once allocations succeed;
+* a zero initial state in imaginary time: the Gram-Schmidt norm collapse (QuantumND_imag.c:297-304)
+  as QND_ENORM;
+* a truncated OUTPUT_IMAG: the real-time driver stops with the reference's read error and exit 1.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_refused_allocation_is_enomem_and_the_context_recovers(qnd_lib, monkeypatch):
+    from tdse_nd_mpi_b200 import Grid, QndError
+
+    shape, dr = (1024, 1024), (0.2, 0.2)
+    grid = Grid(2, shape, dr, "BM4", 0.05)
+    grid.set_potential("H_2D")
+    st = grid.state(O.smooth_state(shape, dr, 1))
+    monkeypatch.setenv("QND_FAIL_ALLOC_ABOVE", str(1 << 20))
+    with pytest.raises(QndError) as ei:
+        grid.energies(st, 2)             # needs two 16.8 MB scratch states
+    assert ei.value.code == 3 and "QND_FAIL_ALLOC_ABOVE" in str(ei.value)
+    monkeypatch.delenv("QND_FAIL_ALLOC_ABOVE")
+    got = grid.energies(st, 2)
+    fresh = Grid(2, shape, dr, "BM4", 0.05)
+    fresh.set_potential("H_2D")
+    np.testing.assert_array_equal(got, fresh.energies(fresh.state(O.smooth_state(shape, dr, 1)), 2))
+
+
+def test_zero_initial_state_collapses_in_imaginary_time(qnd_lib):
+    from tdse_nd_mpi_b200 import Grid, QndError
+
+    grid = Grid(1, (256,), (0.2,), "BM4", 0.05)
+    grid.set_potential("H_1D")
+    states = [grid.state(np.zeros(256, dtype=np.complex128))]
+    with pytest.raises(QndError) as ei:
+        grid.imag_propagate(states, 0, 3)
+    assert ei.value.code == 4 and "norm" in str(ei.value)
+
+
+def test_truncated_output_imag_stops_the_real_driver(qnd_lib, tmp_path):
+    from tdse_nd_mpi_b200.build import build_drivers
+
+    build_drivers()
+    exe = os.path.join(ROOT, "tdse_nd_mpi_b200", "QuantumND_real")
+    head = b"DIMENSION\t1\nN_STATES\t2\nNR\t256\nDR\t0.2\nPOTENTIAL\tH_1D\nE\t\t-0.5\t-0.1\nDE\t0\t0\nPSI\n"
+    (tmp_path / "output.imag").write_bytes(head + bytes(16 * 300))   # state 2 of 256 points is cut short
+    params = ("OUTPUT_IMAG\toutput.imag\nNR\t\t512\nN_STATES\t2\nJ_STATES\t1 2\nCOEFFS_STATES\t1. 1.\nCAP\t\t.1 20.\n"
+              "GAUGE\t\tlength\nN_MODES\t\t1\nINTENSITY\t1.e13\nLAMBDA\t\t800\nELLIPTICITY\t0.\nCEP\t\t0.\n"
+              "DELAY\t\t0.\nENVELOPE\tcos2\nDURATION\t40.\nINTEGRATOR\tBM4\nDT\t\t.1\nTINTEGRATION\t2\n"
+              "DT_SAVE\t\t1.\nN_OBSERVABLES\t1\nOBSERVABLES\tdipole_r\nP_MAX\t\t3.\nR_MASK\t\t5. 10.\nDE\t\t.05\n"
+              "NE\t\t40\n")
+    (tmp_path / "params.real").write_text(params)
+    r = subprocess.run([exe, "params.real"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 1
+    assert "MPI Read Error during chunking" in r.stdout + r.stderr
