@@ -409,3 +409,23 @@ def test_final_spectra_vs_reference(Grid, shape, dr, pot, rmask, prmax):
     live = dens > 1e-10 * dens.max()
     dphi = np.angle(np.exp(1j * (pmd[live, 1] - data[live, 1])))
     assert np.max(np.abs(dphi)) < 1e-8
+
+
+@pytest.mark.parametrize("shape,dr", [((128, 128), (0.3, 0.3)), ((16, 16, 32), (0.5, 0.5, 0.4)), ((4096,), (0.1,))])
+def test_masked_velocity_run_with_all_observables_vs_oracle(Grid, shape, dr):
+    """Velocity gauge with CAP, step mask and every observable (norm, dipole_r, dipole_v with the
+    step's A(t) shift, energy, Lz, accel) each step, against the oracle."""
+    grid, o = _masked_pair(Grid, shape, dr)
+    dim = len(shape)
+    psi0 = O.smooth_state(shape, dr, 18)
+    nsteps = 4
+    rng = np.random.default_rng(19)
+    A = rng.standard_normal((nsteps, grid.s, dim)) * 0.3
+    alpha = rng.standard_normal((nsteps, dim)) * 0.2
+    names = ["norm", "dipole_r", "dipole_v", "energy", "Lz", "accel"]
+    a = psi0.copy()
+    ob_o = o.run_velocity(a, A, alpha, names)
+    st = grid.state(psi0)
+    ob_g = grid.run_velocity(st, A, alpha, names)
+    assert rel(st.download(), a) < TOL
+    np.testing.assert_allclose(ob_g, ob_o, rtol=1e-11, atol=1e-13)
