@@ -429,3 +429,31 @@ def test_masked_velocity_run_with_all_observables_vs_oracle(Grid, shape, dr):
     ob_g = grid.run_velocity(st, A, alpha, names)
     assert rel(st.download(), a) < TOL
     np.testing.assert_allclose(ob_g, ob_o, rtol=1e-11, atol=1e-13)
+
+
+@pytest.mark.parametrize("shape", [(2, 64), (64, 2), (2, 2, 2), (2, 8, 256), (4096, 16), (16, 4096), (2, 4096)])
+def test_extreme_axis_lengths_vs_oracle(Grid, shape):
+    """The shortest (2) and longest (4096) pass axes, strided and contiguous, in 2-D and 3-D: imaginary
+    time and length-gauge steps with observables against the oracle."""
+    dim = len(shape)
+    dr = (0.3,) * dim
+    grid = Grid(dim, shape, dr, "BM4", 0.05)
+    grid.set_potential(POT[{1: "1d", 2: "2d", 3: "3d"}[dim]])
+    grid.set_cap(0.1, 0.5)
+    o = O.OracleCtx(dim, shape, dr, "BM4", 0.05)
+    o.set_potential(POT[{1: "1d", 2: "2d", 3: "3d"}[dim]])
+    o.set_cap(0.1, 0.5)
+    psi0 = O.seeded_state(shape, 21, float(np.prod(dr)))
+    a = psi0.copy()
+    o.step_imag(a, 2)
+    st = grid.state(psi0)
+    grid.integration_step_imag(st, 2)
+    assert rel(st.download(), a) < TOL
+    E = np.random.default_rng(22).standard_normal((3, grid.s, dim)) * 0.05
+    names = ["norm", "dipole_r", "dipole_v", "energy"]
+    a = psi0.copy()
+    ob_o = o.run_length(a, E, names)
+    st.upload(psi0)
+    ob_g = grid.run_length(st, E, names)
+    assert rel(st.download(), a) < TOL
+    np.testing.assert_allclose(ob_g, ob_o, rtol=1e-11, atol=1e-12)
