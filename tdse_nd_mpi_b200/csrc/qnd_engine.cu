@@ -13,6 +13,7 @@
 // sandwich. One sub-step therefore costs one read and one write of the state per
 // axis, and the observables at step boundaries (QuantumND_real.c:197-212) come out
 // of the last pass's fused reductions without the reference's extra transforms.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -24,6 +25,7 @@
 #include <atomic>
 #include <map>
 #include <set>
+#include <tuple>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -168,6 +170,9 @@ struct qnd_ctx {
     DevBuf scratch_a, scratch_b;
     DevBuf spec_rank, spec_partials, spec_out;  // final spectra: per-axis ranks, partial sums, results
     DevBuf field_out, embed_src;                // qnd_field_samples host-output staging; qnd_state_embed source
+    DevBuf err_flag;                            // set by a kernel whose bounded wait ran out
+    DevBuf tune_buf;                            // scratch state of the staging autotuner
+    std::map<std::tuple<const void*, int, int>, CUtensorMap> tmaps;  // strided-pass TMA views of states
 
     // A 1-D axis longer than one pass handles: N = n1 n2 (n1 >= 16, n2 <= 4096) as a virtual
     // n1 x n2 grid transformed in four steps (long_fft). tw_long[v]: the stage twiddles of the
@@ -505,6 +510,7 @@ struct PassSpec {
     const double* apply_vtab = nullptr;
     RedDesc red{};
     int spec_full = 0;           // spec: a full-grid table in line-major order
+    int force_staging = -1;      // strided passes: -1 the tuned staging, 0 per-thread copies, 1 TMA boxes
     // a pass over a virtual axis of a long 1-D axis: its length, log2 stride and stage twiddles
     int vL = 0, vlog2S = 0;
     const void* vtw = nullptr;
@@ -556,11 +562,149 @@ template <typename R> static void fill_args(qnd_ctx* c, const PassSpec& ps, Pass
     a.apply_vtab = ps.apply_vtab;
     a.seed = uint32_t(c->kernels_launched) * 0x9e3779b9u + 0x632be5abu;
     a.red = ps.red;
+    a.err = c->err_flag.as<int>();
 }
 
 struct LaunchCfg {
     int blocks_per_sm = 0;
 };
+
+// cuTensorMapEncodeTiled from the driver, found at run time (the library links only the runtime).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn tensor_map_encoder() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// The TMA view of a state for a strided pass along an axis of L points with stride S = 2^log2S:
+// a 3-D tensor {S (contiguous sub-index), L, n / (S L)} of complex values (FP64: pairs of doubles;
+// FP32: one 8-byte element each) whose boxes {G lines, min(L, 256) rows, 1} are a CTA's lines. False
+// (per-thread staging) unless the boxes obey the rules of the copy engine: a 16-byte aligned base,
+// 16-byte box rows and x offsets (G complex values a multiple of 16 bytes), and full groups of G
+// lines that share their outer index (G <= S, every group complete).
+static bool strided_tma_map(qnd_ctx* c, const void* psi, int L, int log2S, int G, CUtensorMap* map) {
+    if (std::getenv("QND_NO_TMA")) return false;
+    const int64_t S = int64_t(1) << log2S;
+    const size_t ce = c->elem();
+    if (reinterpret_cast<uintptr_t>(psi) % 16 || S < G || (size_t(G) * ce) % 16 || (c->n / L) % G) return false;
+    const auto key = std::make_tuple(psi, L, log2S);
+    auto it = c->tmaps.find(key);
+    if (it != c->tmaps.end()) {
+        *map = it->second;
+        return true;
+    }
+    EncodeTiledFn enc = tensor_map_encoder();
+    if (!enc) return false;
+    const int boxl = L < 256 ? L : 256;
+    cuuint64_t dims[3] = {cuuint64_t(c->fp64 ? 2 * S : S), cuuint64_t(L), cuuint64_t(c->n / (S * L))};
+    cuuint64_t strides[2] = {cuuint64_t(S) * ce, cuuint64_t(S) * cuuint64_t(L) * ce};
+    cuuint32_t box[3] = {cuuint32_t(c->fp64 ? 2 * G : G), cuuint32_t(boxl), 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUtensorMap m;
+    const CUresult r = enc(&m, c->fp64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_UINT64, 3,
+                           const_cast<void*>(psi), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return false;
+    if (c->tmaps.size() >= 64) c->tmaps.clear();
+    c->tmaps[key] = m;
+    *map = m;
+    return true;
+}
+
+static void launch_pass(qnd_ctx* c, const PassSpec& ps);
+
+// Staging autotuner. A strided pass can stage its CTA's lines by per-thread cp.async copies or by
+// TMA box loads; both move the same values into the same registers, so the choice changes the time
+// and never the results. Per (device, precision, points, line length, stride) the first eligible
+// launch outside a stream capture times a forward-transform pass along that geometry with each
+// staging (one warm-up and three timed launches each, on a zeroed scratch state, untimed by the
+// launch counters) and keeps TMA only if it is at least 2% faster. Until then, and with QND_TUNE=0,
+// lines of 1024 points and more use TMA (measured faster there, slower at 256).
+struct StagingKey {
+    int device, fp64;
+    long long n;
+    int L, log2S;
+    bool operator<(const StagingKey& o) const {
+        return std::tie(device, fp64, n, L, log2S) < std::tie(o.device, o.fp64, o.n, o.L, o.log2S);
+    }
+};
+static std::mutex g_staging_mu;
+static std::map<StagingKey, int> g_staging;
+
+static int staging_choice(qnd_ctx* c, const PassSpec& ps, int L, int log2S) {
+    const StagingKey key{c->device, int(c->fp64), c->n, L, log2S};
+    {
+        std::lock_guard<std::mutex> lk(g_staging_mu);
+        auto it = g_staging.find(key);
+        if (it != g_staging.end()) return it->second;
+    }
+    const int fallback = L >= 1024 ? 1 : 0;
+    const char* tune = std::getenv("QND_TUNE");
+    if ((tune && !std::atoi(tune)) || c->profiling) return fallback;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    QND_CK(cudaStreamIsCapturing(c->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return fallback;
+    c->tune_buf.ensure(size_t(c->n) * c->elem());
+    QND_CK(cudaMemsetAsync(c->tune_buf.p, 0, size_t(c->n) * c->elem(), c->stream));
+    CUtensorMap probe;
+    const PassKernelInfo info = lookup_pass(c->fp64, L, true, PM_FFT_FWD);
+    int choice = 0;
+    if (strided_tma_map(c, c->tune_buf.p, L, log2S, info.G, &probe)) {
+        PassSpec t;
+        t.axis = ps.axis;
+        t.mode = PM_FFT_FWD;
+        t.psi = c->tune_buf.p;
+        t.vL = ps.vL;
+        t.vlog2S = ps.vlog2S;
+        t.vtw = ps.vtw;
+        const int64_t k0 = c->kernels_launched;
+        cudaEvent_t e0, e1;
+        QND_CK(cudaEventCreate(&e0));
+        QND_CK(cudaEventCreate(&e1));
+        float ms[2] = {0.f, 0.f};
+        for (int mode = 0; mode < 2; ++mode) {
+            t.force_staging = mode;
+            launch_pass(c, t);
+            QND_CK(cudaEventRecord(e0, c->stream));
+            for (int r = 0; r < 3; ++r) launch_pass(c, t);
+            QND_CK(cudaEventRecord(e1, c->stream));
+            QND_CK(cudaEventSynchronize(e1));
+            QND_CK(cudaEventElapsedTime(&ms[mode], e0, e1));
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        c->kernels_launched = k0;
+        choice = ms[1] < 0.98f * ms[0] ? 1 : 0;
+    }
+    std::lock_guard<std::mutex> lk(g_staging_mu);
+    g_staging[key] = choice;
+    return choice;
+}
+
+// Reads and clears the error flag that a kernel sets when a bounded wait ran out.
+static void check_device_error(qnd_ctx* c) {
+    if (!c->err_flag.p) return;
+    int flag = 0;
+    QND_CK(cudaMemcpyAsync(&flag, c->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    QND_CK(cudaStreamSynchronize(c->stream));
+    if (flag) {
+        QND_CK(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), c->stream));
+        QND_FAIL(QND_ECUDA, "a pass kernel's wait for its TMA box loads ran out (results of that call are invalid)");
+    }
+}
 
 // Launch one fused axis pass: persistent grid (at most the resident CTAs), programmatic
 // dependent launch so the pass's prologue overlaps the tail of the previous kernel.
@@ -573,6 +717,7 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     const PassKernelInfo info = lookup_pass(c->fp64, L, strided, ps.mode);
     const long long nlines = c->n / L;
     const long long ngroups = (nlines + info.G - 1) / info.G;
+    const int staging = !strided ? 0 : ps.force_staging >= 0 ? ps.force_staging : staging_choice(c, ps, L, log2S);
     static std::map<std::pair<const void*, int>, LaunchCfg> configured;  // per (kernel, device)
     auto cfg_key = std::make_pair(info.fn, c->device);
     auto cfg_it = configured.find(cfg_key);
@@ -619,6 +764,7 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         a.tw = static_cast<const double2*>(tw);
         a.log2S = log2S;
         a.nlines = nlines;
+        if (strided && staging) a.use_tma = strided_tma_map(c, ps.psi, L, log2S, info.G, &a.tmap) ? 1 : 0;
         void* args[] = {&a};
         QND_CK(cudaLaunchKernelExC(&lc, info.fn, args));
     } else {
@@ -628,6 +774,7 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         a.tw = static_cast<const float2*>(tw);
         a.log2S = log2S;
         a.nlines = nlines;
+        if (strided && staging) a.use_tma = strided_tma_map(c, ps.psi, L, log2S, info.G, &a.tmap) ? 1 : 0;
         void* args[] = {&a};
         QND_CK(cudaLaunchKernelExC(&lc, info.fn, args));
     }
@@ -1540,6 +1687,7 @@ static void run_realtime(qnd_ctx* c, void* psi, const double* field_host, const 
         }
     }
     QND_CK(cudaGetLastError());
+    if (nv > 0) check_device_error(c);  // the rows were read back: the call synchronised anyway
 }
 
 // ---------------------------------------------------------------- adjoint --
@@ -1899,6 +2047,8 @@ static void build_context(qnd_ctx* c, int dim, const int64_t* nr, const double* 
         rall.insert(rall.end(), c->r[j].begin(), c->r[j].end());
         pall.insert(pall.end(), c->p[j].begin(), c->p[j].end());
     }
+    c->err_flag.ensure(sizeof(int));
+    QND_CK(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), c->stream));
     upload_f64(c, c->r_dev, rall);
     upload_f64(c, c->p_dev, pall);
     if (dim == 1 && nr[0] > 4096) {
@@ -2186,6 +2336,7 @@ int qnd_state_download(qnd_ctx* ctx, double* host, const void* psi_dev) {
         QND_CK(cudaStreamSynchronize(ctx->stream));
         for (int64_t i = 0; i < 2 * ctx->n; ++i) host[i] = double(f[i]);
     }
+    check_device_error(ctx);
     QND_API_END
 }
 
@@ -2195,6 +2346,7 @@ int qnd_synchronize(qnd_ctx* ctx) {
     set_device(ctx);
     QND_CK(cudaStreamSynchronize(ctx->stream));
     QND_CK(cudaGetLastError());
+    check_device_error(ctx);
     QND_API_END
 }
 

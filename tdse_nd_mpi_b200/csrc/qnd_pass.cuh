@@ -28,6 +28,8 @@
 // to finish (ticket counter) adds the partials in a fixed order.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (the type only; maps are encoded on the host)
+
 #include "qnd_fft.cuh"
 
 namespace qnd {
@@ -88,6 +90,12 @@ template <typename R> struct PassArgs {
     unsigned seed;               // FP32: the random stream of the stochastic rounding (one per launch)
     const double* apply_vtab;
     RedDesc red;
+    // strided passes: the state as a 3-D tensor {contiguous sub-index, pass axis, outer} for TMA box
+    // loads of a CTA's G lines (use_tma = 0: per-thread cp.async staging); err: set when a wait for
+    // those loads runs out
+    int use_tma;
+    int* err;
+    CUtensorMap tmap;
 };
 
 // Threads-per-line, values-per-thread and lines-per-CTA for a line length.
@@ -114,7 +122,8 @@ template <typename R, int L> struct PassShape {
     // stage twiddles in shared memory when they are small and shared by several lines of the CTA;
     // otherwise read them through L1 (one copy per SM instead of one per CTA)
     static constexpr bool TW_SMEM = G > 1 && size_t(TWN_RAW) * sizeof(cplx_t<R>) <= 16 * 1024;
-    static constexpr int TWN = TW_SMEM ? TWN_RAW : 0;
+    // the line buffers start on a 128-byte boundary (TMA box destinations)
+    static constexpr int TWN = TW_SMEM ? ((TWN_RAW * int(sizeof(cplx_t<R>)) + 127) / 128 * 128) / int(sizeof(cplx_t<R>)) : 0;
     static constexpr size_t SMEM = sizeof(cplx_t<R>) * (size_t(TWN) + size_t(G) * LS);
     // 128-thread CTAs: <= 128 registers (4 CTAs per SM) when shared memory allows; one-line CTAs
     // of L >= 1024 keep their registers (the SM holds as many lines as its register file allows)
@@ -152,6 +161,42 @@ template <typename V> __device__ __forceinline__ void cp_async_elem(V* smem_dst,
     }
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+// ---- TMA box loads completing on an mbarrier (strided passes)
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{\n"
+        ".reg .pred p;\n"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n"
+        "}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// Waits for phase `phase` of the barrier at most `limit` tries; false when they run out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, int limit) {
+    for (int i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
 template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 template <typename R, typename V>
@@ -370,7 +415,7 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
     using SH = PassShape<R, L>;
     constexpr int E = SH::E, T = SH::T, G = SH::G, NT = SH::NT, LS = SH::LS;
     constexpr bool TWS = SH::TW_SMEM;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     V* tw_s = reinterpret_cast<V*>(smem_raw);   // [TWN] stage twiddles (when they fit)
     V* lines = tw_s + SH::TWN;                   // [G][LS]
 
@@ -415,18 +460,46 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
 
     V v[E];
     if constexpr (STRIDED) {
-        // stage the CTA's G neighbouring lines: consecutive threads -> consecutive addresses
-#pragma unroll 4
-        for (int e = t; e < G * L; e += NT) {
-            const int wl = e % G, m = e / G;
-            const long long l2 = g * G + wl;
-            if (l2 < nlines) cp_async_elem(lines + wl * LS + spad<E>(m), a.psi + line_base(l2) + ((long long)m << log2S));
-        }
-        cp_async_commit();
-        cp_async_wait<0>();
-        __syncthreads();
+        if (a.use_tma) {
+            // the CTA's G lines as L/BOXL boxes {G lines, BOXL rows} in [row][line] order, loaded by TMA
+            // (the host enables this only when every group is full and the boxes meet the 16-byte rules)
+            __shared__ __align__(8) uint64_t tma_bar;
+            constexpr int BOXL = L < 256 ? L : 256;
+            const long long lam0 = g * G;
+            if (t == 0) {
+                mbar_init(&tma_bar, 1);
+                mbar_init_fence();
+            }
+            __syncthreads();
+            if (t == 0) {
+                mbar_expect_tx(&tma_bar, uint32_t(G * L * sizeof(V)));
+                const int x = int(lam0 & smask) * int(sizeof(V) / sizeof(uint64_t));
+                const int z = int(lam0 >> log2S);
+#pragma unroll 1
+                for (int c = 0; c < L / BOXL; ++c) tma_load_3d(lines + c * BOXL * G, &a.tmap, x, c * BOXL, z, &tma_bar);
+            }
+            if (!mbar_wait_bounded(&tma_bar, 0, 1 << 20)) {
+                if (tid == 0 && a.err) atomicExch(a.err, 1);
+                mbar_wait_bounded(&tma_bar, 0, 1 << 20);  // still give the copies in flight their time
+            }
 #pragma unroll
-        for (int u = 0; u < E; ++u) v[u] = active ? line[spad<E>(tid + u * T)] : V{R(0), R(0)};
+            for (int u = 0; u < E; ++u) v[u] = lines[(tid + u * T) * G + w];
+            __syncthreads();  // every line has read its inputs before the exchanges reuse the buffer
+        } else {
+            // stage the CTA's G neighbouring lines: consecutive threads -> consecutive addresses
+#pragma unroll 4
+            for (int e = t; e < G * L; e += NT) {
+                const int wl = e % G, m = e / G;
+                const long long l2 = g * G + wl;
+                if (l2 < nlines)
+                    cp_async_elem(lines + wl * LS + spad<E>(m), a.psi + line_base(l2) + ((long long)m << log2S));
+            }
+            cp_async_commit();
+            cp_async_wait<0>();
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < E; ++u) v[u] = active ? line[spad<E>(tid + u * T)] : V{R(0), R(0)};
+        }
     } else {
         const V* __restrict__ src = a.psi;
 #pragma unroll
@@ -440,7 +513,9 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
             apply_factors<R, E, T>(v, tid, base, lbase, a.pro_real, a.pro_cplx, a.ax_in_prologue ? a.ax_cplx : nullptr,
                                    nullptr, a.axis, a.dim, a.shift, a.nmask, a.pro_scale_dev, key0 ^ 0x51ed270bu);
     }
-    if constexpr (STRIDED) lsync();  // staged inputs read before the exchanges reuse the buffer
+    if constexpr (STRIDED) {
+        if (!a.use_tma) lsync();  // staged inputs read before the exchanges reuse the buffer
+    }
 
     double acc[MAX_RED];
 #pragma unroll

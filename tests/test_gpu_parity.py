@@ -457,3 +457,33 @@ def test_extreme_axis_lengths_vs_oracle(Grid, shape):
     ob_g = grid.run_length(st, E, names)
     assert rel(st.download(), a) < TOL
     np.testing.assert_allclose(ob_g, ob_o, rtol=1e-11, atol=1e-12)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("shape,dr", [((1024, 1024), (0.2, 0.2)), ((64, 64, 64), (0.4, 0.4, 0.4)), ((65536,), (0.05,))])
+def test_staging_choice_never_changes_results(Grid, monkeypatch, precision, shape, dr):
+    """Strided passes stage their lines by TMA boxes or by per-thread copies, whichever the staging
+    autotuner measured faster; both paths must give bit-identical states and observables."""
+    dim = len(shape)
+
+    def run():
+        grid, _ = _masked_pair(Grid, shape, dr)
+        gm = grid if precision == "fp64" else None
+        if gm is None:
+            gm = Grid(dim, shape, dr, "BM4", 0.05, precision="mixed")
+            V, grads = soft_coulomb(gm, 0.64)
+            gm.set_potential(V)
+            gm.set_cap(0.05, 2.0)
+            for j in range(dim):
+                gm.set_gradv(j, grads[j])
+                gm.set_mask_axis(j, cos8_mask(gm.axis_r(j)))
+        st = gm.state(O.smooth_state(shape, dr, 23))
+        E = np.random.default_rng(24).standard_normal((5, gm.s, dim)) * 0.05
+        obs = gm.run_length(st, E, ["norm", "dipole_r", "accel"])
+        return obs, st.download()
+
+    tuned = run()
+    monkeypatch.setenv("QND_NO_TMA", "1")
+    copies = run()
+    np.testing.assert_array_equal(tuned[0], copies[0])
+    np.testing.assert_array_equal(tuned[1], copies[1])
