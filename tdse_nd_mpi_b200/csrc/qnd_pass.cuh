@@ -184,6 +184,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
         : "memory");
     return ok != 0;
 }
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* src, int x, int y, int z) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(smem_u32(src)), "r"(x), "r"(y), "r"(z)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// shared memory of the committed bulk stores read (the CTA may then leave; the writes complete
+// before the grid does)
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// generic-proxy writes to shared memory visible to the bulk-copy (async) proxy
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 // Waits for phase `phase` of the barrier at most `limit` tries; false when they run out.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase, int limit) {
     for (int i = 0; i < limit; ++i)
@@ -601,16 +614,35 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
 
     if (store_out) {
         if constexpr (STRIDED) {
-            // park the line in shared memory, then a coalesced copy-out over the G lines
-            lsync();
+            if (a.use_tma) {
+                // the G lines back in [row][line] order, then one thread stores the boxes
+                constexpr int BOXL = L < 256 ? L : 256;
+                __syncthreads();  // every line is done with its exchange buffer
 #pragma unroll
-            for (int u = 0; u < E; ++u) line[spad<E>(tid + u * T)] = v[u];
-            __syncthreads();
+                for (int u = 0; u < E; ++u) lines[(tid + u * T) * G + w] = v[u];
+                fence_proxy_async_smem();
+                __syncthreads();
+                if (t == 0) {
+                    const long long lam0 = g * G;
+                    const int x = int(lam0 & smask) * int(sizeof(V) / sizeof(uint64_t));
+                    const int z = int(lam0 >> log2S);
+#pragma unroll 1
+                    for (int c = 0; c < L / BOXL; ++c) tma_store_3d(&a.tmap, lines + c * BOXL * G, x, c * BOXL, z);
+                    bulk_commit();
+                    bulk_wait_read_all();
+                }
+            } else {
+                // park the line in shared memory, then a coalesced copy-out over the G lines
+                lsync();
+#pragma unroll
+                for (int u = 0; u < E; ++u) line[spad<E>(tid + u * T)] = v[u];
+                __syncthreads();
 #pragma unroll 4
-            for (int e = t; e < G * L; e += NT) {
-                const int wl = e % G, m = e / G;
-                const long long l2 = g * G + wl;
-                if (l2 < nlines) a.psi[line_base(l2) + ((long long)m << log2S)] = lines[wl * LS + spad<E>(m)];
+                for (int e = t; e < G * L; e += NT) {
+                    const int wl = e % G, m = e / G;
+                    const long long l2 = g * G + wl;
+                    if (l2 < nlines) a.psi[line_base(l2) + ((long long)m << log2S)] = lines[wl * LS + spad<E>(m)];
+                }
             }
         } else if (active) {
             V* __restrict__ out = a.psi;
