@@ -182,6 +182,10 @@ int qnd_run_length_batch(int count, qnd_ctx *const *ctxs, void *const *psi_r_dev
  *      NULL. Synchronises. */
 int qnd_adjoint_length(qnd_ctx *ctx, const void *psi0_dev, const double *E_host, int64_t nsteps, const double *w_host,
                        int64_t checkpoint, double *J_out, double *grad_host, void *psiT_dev);
+/* The same for a velocity-gauge run (qnd_step_velocity's steps, the step mask after each): dJ/dA for
+ * every vector-potential sample A_host [nsteps][s][dim]. */
+int qnd_adjoint_velocity(qnd_ctx *ctx, const void *psi0_dev, const double *A_host, int64_t nsteps,
+                         const double *w_host, int64_t checkpoint, double *J_out, double *grad_host, void *psiT_dev);
 
 /* ---- laser field on the device: replaces Initialize_field_vectors (integrators.c:74-101) and
  *      Field_vectors (parameters.c:899-949).

@@ -1,9 +1,10 @@
-"""FP64 CPU adjoint of the length-gauge split-operator run — TEST INFRASTRUCTURE ONLY.
+"""FP64 CPU adjoints of the split-operator runs (length and velocity gauge) — TEST INFRASTRUCTURE ONLY.
 
-The reference has no adjoint; this is the CPU restatement the engine's qnd_adjoint_length is
-checked against (numpy FFTs, FP64), itself checked two ways by the tests: its forward run against
-the C oracle's length-gauge run (pinned to the reference's Integration_step_length,
-integrators.c:170-194), and its gradient against central finite differences of its own J.
+The reference has no adjoint; these are the CPU restatements the engine's qnd_adjoint_length and
+qnd_adjoint_velocity are checked against (numpy FFTs, FP64), themselves checked two ways by the
+tests: their forward runs against the C oracle's length- and velocity-gauge runs (pinned to the
+reference's Integration_step_length / _velocity, integrators.c:170-232), and their gradients
+against central finite differences of their own J.
 
 A length-gauge step on the r-space state (integrators.c:170-194 with the unitary transforms at
 either end folded away) is the operator product
@@ -107,4 +108,62 @@ class LengthRun:
                     grad[k, i, j] = 2.0 * self.h(i) * float(np.sum(self.X[j] * cross))
                 lam = np.conj(self.D(i, E[k])) * lam
                 lam = self.K(lam, -self.c(i))
+        return J, grad
+
+
+class VelocityRun(LengthRun):
+    """Velocity gauge (integrators.c:201-232 on the r-space state): per step
+        psi <- M V(a_{2s-1}) P_{s-1} V(a_{2s-2}) V(a_{2s-3}) ... P_0 V(a_0) psi,
+        V(a) = exp(min(700, -a Vcap)) exp(-i a V),
+        P_i = F^-1 exp(-i h_i sum_j (p_j^2/2 + (p_j + A_j/2) A_j)) F,  A = A[k][i].
+    For J = dNr sum_x w |psi_T|^2 the sample A[k][i][j] contributes
+        dJ/dA[k][i][j] = 2 h_i sum_k (p_j + A_j) Im(conj(lam~') psi~')
+    with unitary transforms of the state and the adjoint state just after P_i."""
+
+    def __init__(self, *args, **kw):
+        super().__init__(*args, **kw)
+        _, ps = grid_axes(self.shape, self.dr)
+        self.P = np.meshgrid(*ps, indexing="ij")
+
+    def vfac(self, a):
+        return np.exp(np.minimum(MAX_EXP_ARG, -a * self.Vcap)) * np.exp(-1j * a * self.V)
+
+    def Pk(self, i, Ak):
+        ph = self.kin + sum((self.P[j] + 0.5 * Ak[i][j]) * Ak[i][j] for j in range(self.dim))
+        return np.exp(-1j * self.h(i) * ph)
+
+    def step(self, psi, Ak, keep=None):
+        for i in range(self.s):
+            psi = self.vfac(self.a[2 * i]) * psi
+            psi = np.fft.ifftn(self.Pk(i, Ak) * np.fft.fftn(psi))
+            if keep is not None:
+                keep.append(psi)
+            psi = self.vfac(self.a[2 * i + 1]) * psi
+        if self.M is not None:
+            psi = self.M * psi
+        return psi
+
+    def adjoint(self, psi0, A, w):
+        A = np.asarray(A, dtype=np.float64)
+        n = A.shape[0]
+        starts = [np.asarray(psi0, dtype=np.complex128).reshape(self.shape)]
+        for k in range(n):
+            starts.append(self.step(starts[-1], A[k]))
+        psiT = starts[-1]
+        J = self.dNr * float(np.sum(w * np.abs(psiT) ** 2))
+        lam = self.dNr * w * psiT
+        grad = np.zeros((n, self.s, self.dim))
+        norm = "ortho"
+        for k in range(n - 1, -1, -1):
+            subs = []
+            self.step(starts[k], A[k], keep=subs)
+            if self.M is not None:
+                lam = self.M * lam
+            for i in range(self.s - 1, -1, -1):
+                lam = np.conj(self.vfac(self.a[2 * i + 1])) * lam
+                cross = np.imag(np.conj(np.fft.fftn(lam, norm=norm)) * np.fft.fftn(subs[i], norm=norm))
+                for j in range(self.dim):
+                    grad[k, i, j] = 2.0 * self.h(i) * float(np.sum((self.P[j] + A[k][i][j]) * cross))
+                lam = np.fft.ifftn(np.conj(self.Pk(i, A[k])) * np.fft.fftn(lam))
+                lam = np.conj(self.vfac(self.a[2 * i])) * lam
         return J, grad

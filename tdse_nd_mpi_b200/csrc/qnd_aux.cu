@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(256) field_tables_kernel(const __grid_constant
         while (ax + 1 < a.dim && pos >= a.off[ax + 1]) ++ax;
         const double f = a.field[blk * a.dim + ax];
         const double x = a.axes[pos];
-        const double h = a.h[ia];
+        const double h = (blk / a.s) >= a.conj_from ? -a.h[ia] : a.h[ia];  // conj: the phase negated
         double theta, mag;
         if (a.velocity) {
             theta = h * (.5 * x * x + (x + .5 * f) * f);

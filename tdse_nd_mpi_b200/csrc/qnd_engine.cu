@@ -374,7 +374,7 @@ static const void* spec_table(qnd_ctx* c, int kind, int ax, double coef) {
     return ptr;
 }
 
-enum RtabKind { RT_IMAG = 0, RT_LENGTH = 1, RT_VEL = 2, RT_LENGTH_ADJ = 3 };
+enum RtabKind { RT_IMAG = 0, RT_LENGTH = 1, RT_VEL = 2, RT_LENGTH_ADJ = 3, RT_VEL_ADJ = 4 };
 static const double NO_COEF = 1e300;  // marks "no second factor"
 
 static inline double clamped_exp(double arg) { return std::exp(arg > MAX_EXP_ARG ? MAX_EXP_ARG : arg); }
@@ -383,7 +383,7 @@ static inline double clamped_exp(double arg) { return std::exp(arg > MAX_EXP_ARG
 //   RT_IMAG   (a[, b]):  exp(min(700, -a V)) [* exp(min(700, -b V))]           real (integrators.c:143-160)
 //   RT_LENGTH (h):       exp(min(700, -h Vcap)) exp(-i h V)                      complex (integrators.c:186-188)
 //   RT_VEL    (a[, b]):  exp(min(700,-a Vcap)) exp(-i a V) [* same with b]       complex (integrators.c:209-229)
-//   RT_LENGTH_ADJ (h):   the complex conjugate of RT_LENGTH (the adjoint of that factor)
+//   RT_LENGTH_ADJ (h), RT_VEL_ADJ (a[, b]): the complex conjugates (the adjoints of those factors)
 // Reorder a full-grid array (comps values per point) to line-major order for axis ax: entry
 // lam*L + m holds point m of line lam (the order in which a pass along ax visits the grid).
 static std::vector<double> line_major(const qnd_ctx* c, const std::vector<double>& nat, int comps, int ax) {
@@ -457,7 +457,7 @@ static const void* rtab(qnd_ctx* c, int kind, double a, double b, int ax) {
                 // FP32 factors are stored as d = w - 1 (one factor, or the product of two)
                 double dr, di;
                 unit_factor_d(-a * vc, a * c->vpot[i], &dr, &di);
-                if (kind == RT_VEL && b != NO_COEF) {
+                if ((kind == RT_VEL || kind == RT_VEL_ADJ) && b != NO_COEF) {
                     double er, ei;
                     unit_factor_d(-b * vc, b * c->vpot[i], &er, &ei);
                     const double pr = dr * er - di * ei, pi = dr * ei + di * er;
@@ -468,7 +468,8 @@ static const void* rtab(qnd_ctx* c, int kind, double a, double b, int ax) {
                 im = di;
             }
             v[2 * i] = re;
-            v[2 * i + 1] = kind == RT_LENGTH_ADJ ? -im : im;  // conj(w), and for FP32 conj(w - 1) = conj(w) - 1
+            // conj(w), and for FP32 conj(w - 1) = conj(w) - 1
+            v[2 * i + 1] = (kind == RT_LENGTH_ADJ || kind == RT_VEL_ADJ) ? -im : im;
         }
         upload_cplx(c, *buf, line_major(c, v, 2, ax));
     }
@@ -1166,8 +1167,10 @@ static void check_imag_clamp(qnd_ctx* c) {
 
 // Per-step field tables (laser phases / velocity-gauge kinetic phases) for a chunk of steps
 // from field samples already on the device.
-static void build_field_tables(qnd_ctx* c, const double* field_dev, int64_t nsteps, bool velocity) {
+static void build_field_tables(qnd_ctx* c, const double* field_dev, int64_t nsteps, bool velocity,
+                               int conj_from = 1 << 30) {
     FieldTableArgs fa{};
+    fa.conj_from = conj_from;
     fa.field = field_dev;
     // velocity tables of a long axis: slot order (k-space tables), the 1/n2 of its sandwich pass
     fa.axes = velocity ? (c->long1d ? c->p_slot_dev.as<double>() : c->p_dev.as<double>()) : c->r_dev.as<double>();
@@ -1188,11 +1191,11 @@ static void build_field_tables(qnd_ctx* c, const double* field_dev, int64_t nste
     QND_CK(cudaGetLastError());
 }
 
-static void upload_field_chunk(qnd_ctx* c, const double* host, int64_t nsteps, bool velocity) {
+static void upload_field_chunk(qnd_ctx* c, const double* host, int64_t nsteps, bool velocity, int conj_from = 1 << 30) {
     const size_t nval = size_t(nsteps) * c->s * c->dim;
     c->field_dev.ensure(nval * 8);
     QND_CK(cudaMemcpyAsync(c->field_dev.p, host, nval * 8, cudaMemcpyHostToDevice, c->stream));
-    build_field_tables(c, c->field_dev.as<double>(), nsteps, velocity);
+    build_field_tables(c, c->field_dev.as<double>(), nsteps, velocity, conj_from);
 }
 
 static const void* field_slice(qnd_ctx* c, int64_t st, int ia, int ax) {
@@ -1692,18 +1695,29 @@ static void run_realtime(qnd_ctx* c, void* psi, const double* field_host, const 
 
 // ---------------------------------------------------------------- adjoint --
 //
-// Gradient of J = dNr sum_x w(x) |psi_T(x)|^2 with respect to every field sample E[k][i][j] of a
-// length-gauge run (an extension: the reference has no adjoint). A step is the operator product
+// Gradient of J = dNr sum_x w(x) |psi_T(x)|^2 with respect to every field sample of a real-time
+// run (an extension: the reference has no adjoint). With the adjoint state lambda = dJ/dconj(psi)
+// (lambda_T = dNr w psi_T), every operator O of the run maps lambda <- O^dagger lambda going
+// backward, and an operator that depends on a sample F contributes 2 Re <lambda', dO/dF psi> with
+// psi' = O psi and lambda' the adjoint state at the same point.
+//
+// Length gauge (integrators.c:170-194 in r-space): a step is
 //   psi <- M K(a_{2s-1}) D_{s-1} K(c_{s-1}) ... D_0 K(c_0) psi,  c_0 = a_0, c_i = a_{2i-1} + a_{2i},
 // with the kinetic sandwiches K(c) (unitary), the step mask M (real, diagonal) and the potential
-// factors D_i = exp(-h_i Vcap) exp(-i h_i (V + x.E[k][i])), h_i = a_{2i} + a_{2i+1} (integrators.c:
-// 170-194 in r-space). With the adjoint state lambda = dJ/dconj(psi) (lambda_T = dNr w psi_T),
-// every operator O maps lambda <- O^dagger lambda going backward, and the factor D_i contributes
-//   dJ/dE[k][i][j] = 2 Re <lambda', -i h_i x_j psi'> = 2 h_i sum_x x_j Im(conj(lambda') psi'),
-// where psi' and lambda' are the state and the adjoint state just after D_i. O^dagger: K(-c) for
-// K(c), M for M, conj(D_i) = RT_LENGTH_ADJ times the laser phases of -E for D_i. The forward states
-// are kept every `every` steps; a segment's step-start states are recomputed from its checkpoint,
-// and a step's sub-step states from its start.
+// factors D_i = exp(-h_i Vcap) exp(-i h_i (V + x.E[k][i])), h_i = a_{2i} + a_{2i+1}, so
+//   dJ/dE[k][i][j] = 2 h_i sum_x x_j Im(conj(lambda') psi')   (just after D_i).
+// Adjoints: K(-c) for K(c), M for M, RT_LENGTH_ADJ times the laser phases of -E for D_i.
+//
+// Velocity gauge (integrators.c:201-232): a step is
+//   psi <- M V(a_{2s-1}) P_{s-1} V(a_{2s-3}) V(a_{2s-2}) ... V(a_1) V(a_2) P_0 V(a_0) psi,
+// with the r-space factors V(a) = exp(-a Vcap) exp(-i a V) and the kinetic sandwiches
+// P_i = F^-1 exp(-i h_i sum_j (p_j^2/2 + (p_j + A_j/2) A_j)) F of the samples A[k][i], so
+// (Parseval, unitary transforms of both states)
+//   dJ/dA[k][i][j] = 2 h_i sum_k (p_j + A[k][i][j]) Im(conj(lambda~') psi~')   (just after P_i).
+// Adjoints: V(a) -> RT_VEL_ADJ, P_i -> the sandwich with the conjugate phase tables.
+//
+// The forward states are kept every `every` steps; a segment's step-start states are recomputed
+// from its checkpoint, and a step's sub-step states from its start.
 
 // psi <- M psi for the step masks set on the axes.
 static void apply_step_masks(qnd_ctx* c, void* psi) {
@@ -1722,17 +1736,32 @@ static void apply_step_masks(qnd_ctx* c, void* psi) {
     QND_CK(cudaGetLastError());
 }
 
+// psi <- t psi for a full-grid complex table in natural order (any dimension).
+static void apply_table(qnd_ctx* c, void* psi, const void* table) {
+    if (c->fp64)
+        launch_point_factors<double>(c->n, static_cast<double2*>(psi), nullptr, static_cast<const double2*>(table),
+                                     nullptr, nullptr, nullptr, c->stream);
+    else
+        launch_point_factors<float>(c->n, static_cast<float2*>(psi), nullptr, static_cast<const float2*>(table),
+                                    nullptr, nullptr, nullptr, c->stream);
+    c->kernels_launched++;
+    QND_CK(cudaGetLastError());
+}
+
 static void copy_state(qnd_ctx* c, void* dst, const void* src) {
     QND_CK(cudaMemcpyAsync(dst, src, size_t(c->n) * c->elem(), cudaMemcpyDeviceToDevice, c->stream));
 }
 
-// Length-gauge steps k0 .. k0+n-1 of the run's field (host [nsteps][s][dim]) on an r-space psi.
-static void length_span(qnd_ctx* c, void* psi, const double* E, int64_t k0, int64_t n, bool masked) {
+// Steps k0 .. k0+n-1 of the run's field samples (host [nsteps][s][dim]) on an r-space psi.
+static void steps_span(qnd_ctx* c, void* psi, const double* F, int64_t k0, int64_t n, bool masked, bool velocity) {
     const int64_t chunk = chunk_steps(c);
     for (int64_t q = 0; q < n; q += chunk) {
         const int64_t ch = std::min(chunk, n - q);
-        upload_field_chunk(c, E + size_t(k0 + q) * c->s * c->dim, ch, false);
-        length_steps(c, psi, 0, ch, RedFn(), masked);
+        upload_field_chunk(c, F + size_t(k0 + q) * c->s * c->dim, ch, velocity);
+        if (!velocity) length_steps(c, psi, 0, ch, RedFn(), masked);
+        else if (!masked) velocity_steps(c, psi, 0, ch, nullptr, false);
+        else  // a velocity chain masks after its last step only: one chain per step
+            for (int64_t k = 0; k < ch; ++k) velocity_steps(c, psi, k, 1, nullptr, true);
     }
 }
 
@@ -1745,19 +1774,23 @@ struct SweepMember {
     double* stage = nullptr;
 };
 
-static void adjoint_length(qnd_ctx* c, const void* psi0, const double* E, int64_t nsteps, const double* w_host,
-                           int64_t every, double* J_out, double* grad_host, void* psiT) {
+static void adjoint_run(qnd_ctx* c, const void* psi0, const double* F, int64_t nsteps, const double* w_host,
+                        int64_t every, double* J_out, double* grad_host, void* psiT, bool velocity) {
     const int s = c->s, d = c->dim;
     const size_t sb = size_t(c->n) * c->elem();
     const int64_t K = std::max<int64_t>(1, std::min(every, nsteps));
     const int64_t nck = (nsteps + K - 1) / K;
     const bool masked = has_mask(c);
-    DevBuf ck, seg, sub, work, lam, wgrid, wscaled, out;
+    DevBuf ck, seg, sub, work, lam, wgrid, wscaled, out, tl, tp;
     ck.ensure(size_t(nck) * sb);
     seg.ensure(size_t(K) * sb);
     sub.ensure(size_t(s) * sb);
     work.ensure(sb);
     lam.ensure(sb);
+    if (velocity) {
+        tl.ensure(sb);
+        tp.ensure(sb);
+    }
     out.ensure((size_t(nsteps) * s * d + 1) * sizeof(double));
     auto at = [&](DevBuf& b, int64_t k) { return static_cast<void*>(static_cast<char*>(b.p) + size_t(k) * sb); };
     // the weight: FP64 for J, and dNr w in the state's precision for lambda_T
@@ -1770,7 +1803,7 @@ static void adjoint_length(qnd_ctx* c, const void* psi0, const double* E, int64_
     copy_state(c, work.p, psi0);
     for (int64_t q = 0; q < nck; ++q) {
         copy_state(c, at(ck, q), work.p);
-        length_span(c, work.p, E, q * K, std::min(K, nsteps - q * K), masked);
+        steps_span(c, work.p, F, q * K, std::min(K, nsteps - q * K), masked, velocity);
     }
     if (psiT) copy_state(c, psiT, work.p);
     double* grad_dev = out.as<double>();
@@ -1798,8 +1831,23 @@ static void adjoint_length(qnd_ctx* c, const void* psi0, const double* E, int64_
         k.coef = coef;
         return std::vector<ChainK>{k};
     };
+    auto kvel = [&](int64_t lst, int ia) {
+        ChainK k;
+        k.kind = KV_FIELD;
+        k.lst = lst;
+        k.ia = ia;
+        return std::vector<ChainK>{k};
+    };
     auto cst = [&](int i) { return i == 0 ? c->as[0] : c->as[2 * i - 1] + c->as[2 * i]; };
     auto hst = [&](int i) { return c->as[2 * i] + c->as[2 * i + 1]; };
+    // velocity gauge: the r-space factor before sandwich i (V(a_0), then V(a_{2i-1}) V(a_{2i}))
+    auto vpre = [&](int i, int kind) {
+        Factor f;
+        f.kind = kind;
+        f.a = i == 0 ? c->as[0] : c->as[2 * i - 1];
+        f.b = i == 0 ? NO_COEF : c->as[2 * i];
+        return f;
+    };
     std::vector<double> fe(size_t(2) * s * d);
     // backward, segment by segment
     for (int64_t q = nck - 1; q >= 0; --q) {
@@ -1807,47 +1855,77 @@ static void adjoint_length(qnd_ctx* c, const void* psi0, const double* E, int64_
         copy_state(c, work.p, at(ck, q));
         for (int64_t k = 0; k < kn; ++k) {
             copy_state(c, at(seg, k), work.p);
-            if (k + 1 < kn) length_span(c, work.p, E, k0 + k, 1, masked);
+            if (k + 1 < kn) steps_span(c, work.p, F, k0 + k, 1, masked, velocity);
         }
         for (int64_t k = kn - 1; k >= 0; --k) {
             const int64_t kk = k0 + k;
-            // field tables of this step: slot 0 the samples (forward), slot 1 their negatives (adjoint)
+            const double* Fk = F + size_t(kk) * s * d;
+            // field tables of this step: slot 0 forward; slot 1 the adjoint's (length: the laser
+            // phases of -E; velocity: the conjugate k-space phases)
             for (int q2 = 0; q2 < s * d; ++q2) {
-                fe[q2] = E[size_t(kk) * s * d + q2];
-                fe[s * d + q2] = -fe[q2];
+                fe[q2] = Fk[q2];
+                fe[s * d + q2] = velocity ? Fk[q2] : -Fk[q2];
             }
-            upload_field_chunk(c, fe.data(), 2, false);
-            // the states just after each D_i
+            upload_field_chunk(c, fe.data(), 2, velocity, velocity ? 1 : (1 << 30));
+            // the states just after each parameter-dependent operator
             copy_state(c, work.p, at(seg, k));
             for (int i = 0; i < s; ++i) {
-                ChainMid post;
-                post.f.kind = RT_LENGTH;
-                post.f.a = hst(i);
-                post.f.laser_ia = i;
-                post.lst = 0;
-                run_chain(c, work.p, kin(cst(i)), {}, Factor{}, 0, nullptr, post);
+                if (velocity) {
+                    run_chain(c, work.p, kvel(0, i), {}, vpre(i, RT_VEL), 0, nullptr, ChainMid{});
+                } else {
+                    ChainMid post;
+                    post.f.kind = RT_LENGTH;
+                    post.f.a = hst(i);
+                    post.f.laser_ia = i;
+                    post.lst = 0;
+                    run_chain(c, work.p, kin(cst(i)), {}, Factor{}, 0, nullptr, post);
+                }
                 copy_state(c, at(sub, i), work.p);
             }
-            // lambda back through M and K(a_{2s-1})
+            // lambda back through the step's last operators: M, then K(a_{2s-1}) or V(a_{2s-1})
             if (masked) apply_step_masks(c, lam.p);
-            run_chain(c, lam.p, kin(-c->as[2 * s - 1]), {}, Factor{}, 0, nullptr, ChainMid{});
+            if (velocity) apply_table(c, lam.p, rtab(c, RT_VEL_ADJ, c->as[2 * s - 1], NO_COEF));
+            else run_chain(c, lam.p, kin(-c->as[2 * s - 1]), {}, Factor{}, 0, nullptr, ChainMid{});
             for (int i = s - 1; i >= 0; --i) {
                 RedDesc rg{};
                 rg.n = d;
+                const void* pr = at(sub, i);
+                const void* pl = lam.p;
+                if (velocity) {
+                    // unitary transforms of both states, weights p_j + A_j
+                    copy_state(c, tl.p, lam.p);
+                    copy_state(c, tp.p, at(sub, i));
+                    unitary_fft(c, tl.p, true);
+                    unitary_fft(c, tp.p, true);
+                    pr = tp.p;
+                    pl = tl.p;
+                    for (int j = 0; j < d; ++j) {
+                        c->wtab_dev[j].ensure(size_t(c->nr[j]) * 8);
+                        launch_axis_table<double>(0, c->p_dev.as<double>() + c->axoff[j], int(c->nr[j]),
+                                                  Fk[size_t(i) * d + j], c->wtab_dev[j].p, c->stream);
+                        c->kernels_launched++;
+                    }
+                }
                 for (int j = 0; j < d; ++j) {
                     rg.kind[j] = RK_BILIN_IM;
                     rg.wkind[j] = WK_AXIS;
                     rg.waxis[j] = j;
-                    rg.wtab[j] = c->r_dev.as<double>() + c->axoff[j];
+                    rg.wtab[j] = velocity ? c->wtab_dev[j].as<double>() : c->r_dev.as<double>() + c->axoff[j];
                     rg.scale[j] = 2.0 * hst(i);
                 }
                 rg.out = grad_dev + (size_t(kk) * s + i) * d;
-                grid_reduce(c, at(sub, i), rg, lam.p);
-                Factor adj;
-                adj.kind = RT_LENGTH_ADJ;
-                adj.a = hst(i);
-                adj.laser_ia = i;
-                run_chain(c, lam.p, kin(-cst(i)), {}, adj, 1, nullptr, ChainMid{});
+                grid_reduce(c, pr, rg, pl);
+                if (velocity) {
+                    ChainMid post;
+                    post.f = vpre(i, RT_VEL_ADJ);
+                    run_chain(c, lam.p, kvel(1, i), {}, Factor{}, 0, nullptr, post);
+                } else {
+                    Factor adj;
+                    adj.kind = RT_LENGTH_ADJ;
+                    adj.a = hst(i);
+                    adj.laser_ia = i;
+                    run_chain(c, lam.p, kin(-cst(i)), {}, adj, 1, nullptr, ChainMid{});
+                }
             }
         }
     }
@@ -1856,6 +1934,7 @@ static void adjoint_length(qnd_ctx* c, const void* psi0, const double* E, int64_
     double J = 0.0;
     QND_CK(cudaMemcpyAsync(&J, J_dev, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     QND_CK(cudaStreamSynchronize(c->stream));
+    check_device_error(c);
     if (J_out) *J_out = J;
 }
 
@@ -2882,7 +2961,23 @@ int qnd_adjoint_length(qnd_ctx* ctx, const void* psi0_dev, const double* E_host,
     QND_NEED(grad_host);
     if (checkpoint < 1) QND_FAIL(QND_EINVAL, "qnd_adjoint_length: checkpoint interval %lld < 1", (long long)checkpoint);
     set_device(ctx);
-    adjoint_length(ctx, psi0_dev, E_host, nsteps, w_host, checkpoint, J_out, grad_host, psiT_dev);
+    adjoint_run(ctx, psi0_dev, E_host, nsteps, w_host, checkpoint, J_out, grad_host, psiT_dev, false);
+    QND_API_END
+}
+
+int qnd_adjoint_velocity(qnd_ctx* ctx, const void* psi0_dev, const double* A_host, int64_t nsteps,
+                         const double* w_host, int64_t checkpoint, double* J_out, double* grad_host, void* psiT_dev) {
+    using namespace qnd;
+    QND_API_BEGIN
+    QND_NEED(ctx);
+    QND_NEED(psi0_dev);
+    QND_NEED(w_host);
+    if (nsteps < 1) QND_FAIL(QND_EINVAL, "qnd_adjoint_velocity: nsteps %lld < 1", (long long)nsteps);
+    QND_NEED(A_host);
+    QND_NEED(grad_host);
+    if (checkpoint < 1) QND_FAIL(QND_EINVAL, "qnd_adjoint_velocity: checkpoint interval %lld < 1", (long long)checkpoint);
+    set_device(ctx);
+    adjoint_run(ctx, psi0_dev, A_host, nsteps, w_host, checkpoint, J_out, grad_host, psiT_dev, true);
     QND_API_END
 }
 

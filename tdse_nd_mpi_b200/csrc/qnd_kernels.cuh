@@ -70,6 +70,7 @@ struct FieldTableArgs {
     int nr[MAX_DIM], off[MAX_DIM], ntot;
     double h[32];
     int velocity;
+    int conj_from;        // steps from this one on get the conjugate factors (adjoint sweeps)
 };
 template <typename R> void launch_field_tables(const FieldTableArgs& a, cplx_t<R>* out, cudaStream_t st);
 

@@ -309,14 +309,22 @@ class Grid:
     def adjoint_length(self, psi0, E, weight, checkpoint=50, psiT=None):
         """J = dNr sum w |psi_T|^2 after the length-gauge steps with field samples E [nsteps, s, dim]
         from psi0 (not modified), and dJ/dE [nsteps, s, dim] by the adjoint (qnd_adjoint_length)."""
-        E = _f64(E)
-        n = E.shape[0]
-        E = self._field(E, n)
+        return self._adjoint(lib().qnd_adjoint_length, psi0, E, weight, checkpoint, psiT)
+
+    def adjoint_velocity(self, psi0, A, weight, checkpoint=50, psiT=None):
+        """The same for velocity-gauge steps with vector-potential samples A: J and dJ/dA
+        (qnd_adjoint_velocity)."""
+        return self._adjoint(lib().qnd_adjoint_velocity, psi0, A, weight, checkpoint, psiT)
+
+    def _adjoint(self, fn, psi0, F, weight, checkpoint, psiT):
+        F = _f64(F)
+        n = F.shape[0]
+        F = self._field(F, n)
         w = _f64(np.broadcast_to(np.asarray(weight, dtype=np.float64), self.shape).copy())
         grad = np.zeros((n, self.s, self.dim))
         J = C.c_double()
-        check(lib().qnd_adjoint_length(self.h, C.c_void_p(_ptr_of(psi0)), _dptr(E), int(n), _dptr(w), int(checkpoint),
-                                       C.byref(J), _dptr(grad), None if psiT is None else C.c_void_p(_ptr_of(psiT))))
+        check(fn(self.h, C.c_void_p(_ptr_of(psi0)), _dptr(F), int(n), _dptr(w), int(checkpoint), C.byref(J), _dptr(grad),
+                 None if psiT is None else C.c_void_p(_ptr_of(psiT))))
         return J.value, grad
 
     # -- laser field and initial state on the device

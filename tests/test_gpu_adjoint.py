@@ -147,3 +147,73 @@ def test_autograd_bridge(Grid):
     J_ref, g_ref = grid.adjoint_length(st, E0, w, checkpoint=2)
     assert float(J.detach()) == J_ref
     np.testing.assert_array_equal(E.grad.numpy(), 2.0 * g_ref)
+
+
+def _vpair(Grid, shape, dr, integ, precision="fp64", masked=True):
+    grid, run, w = _pair(Grid, shape, dr, integ, precision, masked)
+    masks = None
+    if masked:
+        masks = [np.where(np.abs(grid.axis_r(j)) > 0.85 * np.abs(grid.axis_r(j)).max(), 0.98, 1.0)
+                 for j in range(len(shape))]
+    return grid, A.VelocityRun(shape, dr, integ, 0.05, run.V, run.Vcap, masks), w
+
+
+@pytest.mark.parametrize("shape,dr,integ", [((256,), (0.3,), "BM4"), ((64, 64), (0.4, 0.4), "BM4"),
+                                            ((16, 16, 16), (0.6, 0.6, 0.6), "Verlet"), ((8192,), (0.1,), "BM6")])
+def test_velocity_adjoint_matches_cpu_adjoint(Grid, shape, dr, integ):
+    """qnd_adjoint_velocity (dJ/dA of a velocity-gauge run) against the FP64 CPU adjoint."""
+    grid, run, w = _vpair(Grid, shape, dr, integ)
+    psi0 = O.smooth_state(shape, dr, 31)
+    Avec = np.random.default_rng(32).standard_normal((7, grid.s, len(shape))) * 0.3
+    J_ref, g_ref = run.adjoint(psi0, Avec, w)
+    st = grid.state(psi0)
+    out = grid.state()
+    J, g = grid.adjoint_velocity(st, Avec, w, checkpoint=3, psiT=out)
+    assert abs(J - J_ref) <= 1e-11 * abs(J_ref)
+    assert _rel(g, g_ref) < 1e-10
+    assert _rel(out.download(), run.run(psi0, Avec)) < 1e-12
+
+
+def test_velocity_adjoint_matches_finite_differences(Grid):
+    """2-D 128^2 BM4 with the step mask, 60 steps, checkpoints every 16: dJ/dA at 12 random samples
+    against central differences of the engine's own forward run (qnd_run_velocity)."""
+    shape, dr = (128, 128), (0.3, 0.3)
+    grid, _, w = _vpair(Grid, shape, dr, "BM4")
+    psi0 = O.smooth_state(shape, dr, 33)
+    rng = np.random.default_rng(34)
+    Avec = rng.standard_normal((60, grid.s, 2)) * 0.3
+    J, g = grid.adjoint_velocity(grid.state(psi0), Avec, w, checkpoint=16)
+    out = grid.state()
+
+    def objective(Ap):
+        out.upload(psi0)
+        grid.run_velocity(out, Ap)
+        return grid.dNr * float(np.sum(w * np.abs(out.download()) ** 2))
+
+    assert objective(Avec) == pytest.approx(J, rel=1e-12)
+    eps = 1e-5
+    scale = np.abs(g).max()
+    for _ in range(12):
+        idx = (int(rng.integers(0, 60)), int(rng.integers(0, grid.s)), int(rng.integers(0, 2)))
+        Ap, Am = Avec.copy(), Avec.copy()
+        Ap[idx] += eps
+        Am[idx] -= eps
+        fd = (objective(Ap) - objective(Am)) / (2 * eps)
+        assert abs(fd - g[idx]) <= 1e-5 * max(abs(fd), 1e-3 * scale), (idx, fd, g[idx])
+
+
+def test_velocity_autograd_bridge(Grid):
+    import torch
+
+    from tdse_nd_mpi_b200.adjoint import absorbed_weight, velocity_gauge_objective
+
+    grid, _, _ = _vpair(Grid, (64, 64), (0.4, 0.4), "BM4")
+    w = absorbed_weight(grid, 6.0)
+    st = grid.state(O.smooth_state((64, 64), (0.4, 0.4), 35))
+    A0 = np.random.default_rng(36).standard_normal((5, grid.s, 2)) * 0.3
+    Avec = torch.tensor(A0, requires_grad=True)
+    J = velocity_gauge_objective(grid, st, Avec, w, checkpoint=2)
+    J.backward()
+    J_ref, g_ref = grid.adjoint_velocity(st, A0, w, checkpoint=2)
+    assert float(J.detach()) == J_ref
+    np.testing.assert_array_equal(Avec.grad.numpy(), g_ref)
