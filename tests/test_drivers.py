@@ -185,3 +185,98 @@ def test_real_driver_outputs_match_reference_executable(driver, tmp_path, gauge,
     assert w1[:k1] == w2[:k2]
     p1, p2 = np.frombuffer(w1[k1:], np.complex128), np.frombuffer(w2[k2:], np.complex128)
     assert np.linalg.norm(p1 - p2) / np.linalg.norm(p2) < 1e-9
+
+
+# The reference's example inputs (its params.imag and params.real), as a user would run them;
+# TINTEGRATION is shortened through the drivers' own KEY VALUE overrides so that the reference
+# executable finishes in seconds on the host.
+EXAMPLE_IMAG = """OUTPUT_IMAG \toutput.imag
+
+DIMENSION\t1
+N_STATES \t4
+
+POTENTIAL\tH_1D
+
+DR\t\t.2
+NR\t\t512
+
+INTEGRATOR \tBM4
+DT \t\t.1
+TINTEGRATION \t1e3
+"""
+
+EXAMPLE_REAL = """OUTPUT_IMAG\toutput.imag
+
+NR \t\t262144
+
+N_STATES \t1
+J_STATES \t1
+COEFFS_STATES\t1.
+
+CAP \t\t.1\t20.
+
+GAUGE \t\tlength
+N_MODES \t10
+INTENSITY \t1.e11 1.e11 1.e11 1.e11 1.e11 1.e11 1.e11 1.e11 1.e11 1.e11
+LAMBDA \t\t800 88.8888888888889 72.7272727272727 61.5384615384615 53.3333333333333 47.0588235294118 42.1052631578947 38.0952380952381 34.7826086956522 32
+ELLIPTICITY \t0. 0. 0. 0. 0. 0. 0. 0. 0. 0.
+CEP \t\t0. 0. 0. 0. 0. 0. 0. 0. 0. 0.
+DELAY \t\t0. 0. 0. 0. 0. 0. 0. 0. 0. 0.
+ENVELOPE \tcos2 cos2 cos2 cos2 cos2 cos2 cos2 cos2 cos2 cos2
+DURATION \t10000. 10000. 10000. 10000. 10000. 10000. 10000. 10000. 10000. 10000.
+
+INTEGRATOR \tBM4
+DT \t\t.1
+TINTEGRATION \t15000.
+
+DT_SAVE \t1.
+N_OBSERVABLES \t3
+OBSERVABLES \tPED PMD wavefunction
+
+P_MAX \t\t10.
+R_MASK \t\t20. 30.
+DE \t\t.01
+NE \t\t200
+"""
+
+
+@pytest.mark.gpu
+def test_reference_example_inputs_end_to_end(driver, tmp_path):
+    """The reference's own example: imaginary time on 512 points (4 states), then the real-time run
+    on NR 262144 (a four-step long axis) under a 10-mode field, writing PED, PMD and the
+    wavefunction; both stages shortened by TINTEGRATION overrides. Every file against the
+    reference's executables on the same inputs."""
+    from oracle import oracle as O
+
+    if not (os.path.exists(REF_IMAG) and os.path.exists(REF_REAL)):
+        pytest.skip("reference executables not built")
+    out = {}
+    for who, imag, real in (("ours", DRIVER, REAL_DRIVER), ("ref", REF_IMAG, REF_REAL)):
+        d = tmp_path / who
+        d.mkdir()
+        r = run(imag, EXAMPLE_IMAG, d, "TINTEGRATION", "20")
+        assert r.returncode == 0, (who, r.stdout[-1500:], r.stderr[-1500:])
+        (d / "params.real").write_text(EXAMPLE_REAL)
+        r = subprocess.run([real, "params.real", "TINTEGRATION", "3"], cwd=d, capture_output=True, text=True,
+                           timeout=900)
+        assert r.returncode == 0, (who, r.stdout[-1500:], r.stderr[-1500:])
+        out[who] = d
+    t1, h1, psi1 = read_output_imag(out["ours"] / "output.imag")
+    t2, h2, psi2 = read_output_imag(out["ref"] / "output.imag")
+    np.testing.assert_allclose(np.array(h1["E"], float), np.array(h2["E"], float), rtol=1e-11)
+    assert np.linalg.norm(psi1 - psi2) / np.linalg.norm(psi2) < 1e-10
+    for f in ("electric_field.real", "vector_potential.real"):
+        np.testing.assert_allclose(np.loadtxt(out["ours"] / f), np.loadtxt(out["ref"] / f), rtol=1e-12, atol=1e-15)
+    ped1, ped2 = np.loadtxt(out["ours"] / "PED.real"), np.loadtxt(out["ref"] / "PED.real")
+    np.testing.assert_allclose(ped1, ped2, rtol=0, atol=1e-10 * np.abs(ped2[:, 1]).max())
+    (hd1, d1), (hd2, d2) = O.read_pmd(out["ours"] / "PMD.real"), O.read_pmd(out["ref"] / "PMD.real")
+    assert hd1 == hd2 and d1.shape == d2.shape
+    # after 3 a.u. nothing has reached R_MASK: the spectra are at the FP64 rounding floor of a
+    # normalised state (|psi~|^2 ~ 1e-21), so compare the amplitudes to an absolute 1e-13
+    np.testing.assert_allclose(np.sqrt(d1[:, 0]), np.sqrt(d2[:, 0]), rtol=0, atol=1e-13)
+    w1 = open(out["ours"] / "wavefunction.real", "rb").read()
+    w2 = open(out["ref"] / "wavefunction.real", "rb").read()
+    k1, k2 = w1.index(b"PSI_BINARY_START\n") + 17, w2.index(b"PSI_BINARY_START\n") + 17
+    assert w1[:k1] == w2[:k2]
+    p1, p2 = np.frombuffer(w1[k1:], np.complex128), np.frombuffer(w2[k2:], np.complex128)
+    assert p1.size == 262144 and np.linalg.norm(p1 - p2) / np.linalg.norm(p2) < 1e-9
