@@ -211,7 +211,8 @@ def test_gram_schmidt_norm_collapse_is_an_error(Grid):
     assert ei.value.code == 4 and "norm" in str(ei.value)
 
 
-@pytest.mark.parametrize("shape,dr", [((256, 256), (0.2, 0.2)), ((1024, 1024), (0.2, 0.2))])
+@pytest.mark.parametrize("shape,dr", [((256, 256), (0.2, 0.2)), ((1024, 1024), (0.2, 0.2)), ((4096,), (0.1,)),
+                                      ((32, 32, 64), (0.5, 0.5, 0.4))])
 def test_mixed_precision_error_bound(Grid, shape, dr):
     """Complex64 bulk with FP64 reductions: stated bounds against the FP64 oracle after 10 steps:
     wavefunction relative L2 <= 2e-5, observables relative <= 5e-6 (the norm drifts by ~1e-7 per
