@@ -1275,7 +1275,10 @@ static void run_chain(qnd_ctx* c, void* psi, const std::vector<ChainK>& K, const
     const int64_t NK = int64_t(K.size());
     if (NK == 0 || int64_t(M.size()) != NK - 1) QND_FAIL(QND_EINVAL, "internal: malformed sandwich chain");
     if (c->long1d) {
-        // one four-step sandwich per kinetic factor; the r-space work between them element-wise
+        // four-step sandwiches: length-n1 forward, the length-n2 sandwich pass (twiddles, slot-order
+        // k-space table, conjugate twiddles), then either one length-n1 roundtrip pass (inverse,
+        // the r-space factors in natural order, forward of the next sandwich; FP32) or the
+        // length-n1 inverse and element-wise work in natural order (FP64, reductions, chain end)
         auto point = [&](const Factor& f, int64_t lst, bool mask, const double* scale_dev) {
             const void *tr = nullptr, *tc = nullptr;
             const void* axc[MAX_DIM] = {nullptr, nullptr, nullptr};
@@ -1283,11 +1286,30 @@ static void run_chain(qnd_ctx* c, void* psi, const std::vector<ChainK>& K, const
             long_point(c, psi, tr, tc, axc[0], mask ? c->mask_dev[0].p : nullptr, scale_dev);
         };
         point(pre, pre_lst, false, pre_scale);
+        launch_pass(c, long_pass(c, 0, PM_FFT_FWD, psi, 1.0));
         for (int64_t i = 0; i < NK; ++i) {
-            long_sandwich(c, psi, chain_spec(c, K[i], 0));
-            const ChainMid& m = i + 1 < NK ? M[i] : post;
+            PassSpec ps = long_pass(c, 1, PM_SANDWICH, psi, 1.0);
+            ps.pro_cplx = c->twf_long.p;
+            ps.spec = chain_spec(c, K[i], 0);
+            ps.spec_full = 1;
+            ps.epi_cplx = c->twc_long.p;
+            launch_pass(c, ps);
+            const bool last = i + 1 == NK;
+            const ChainMid& m = last ? post : M[i];
+            // the roundtrip gathers its natural-order tables across the strided virtual axis:
+            // measured 13% faster per step in FP32 at 262144 points, 4% slower in FP64 (where the
+            // separate coalesced element-wise kernel wins)
+            if (!last && !m.red && !c->fp64) {
+                PassSpec r = long_pass(c, 0, PM_ROUNDTRIP, psi, 1.0 / double(c->n1));
+                set_factor(c, m.f, 0, m.lst, &r.mid_real, &r.mid_cplx, r.mid_ax_cplx);
+                if (m.mask) r.mid_ax_real[0] = c->mask_dev[0].p;
+                launch_pass(c, r);
+                continue;
+            }
+            launch_pass(c, long_pass(c, 0, PM_FFT_INV, psi, 1.0 / double(c->n1)));
             point(m.f, m.lst, m.mask, nullptr);
             if (m.red) grid_reduce(c, psi, *m.red);
+            if (!last) launch_pass(c, long_pass(c, 0, PM_FFT_FWD, psi, 1.0));
         }
         return;
     }

@@ -23,6 +23,9 @@
 //   PM_SPECRED   reductions of |FFT psi|^2 weighted by k-space tables; no write
 //   PM_APPLY     u = IFFT[spec . FFT psi] (+ V psi) (+ dst); optional store into dst and
 //                reductions of |u|^2 or Re(conj(partner) u)   (energy moments, Lz)
+//   PM_ROUNDTRIP psi <- FFT[ mid(x) . scale . IFFT[psi] ]: the closing inverse transform of one
+//                sandwich and the opening transform of the next on the strided virtual axis of a
+//                long 1-D axis, with the r-space factors between (tables in natural order)
 //
 // Reductions are FP64 and deterministic: per-CTA partial sums, then the last CTA
 // to finish (ticket counter) adds the partials in a fixed order.
@@ -37,7 +40,16 @@ namespace qnd {
 constexpr int MAX_RED = 8;
 constexpr int MAX_DIM = 3;
 
-enum : int { PM_SANDWICH = 0, PM_FFT_FWD = 1, PM_FFT_INV = 2, PM_SPECRED = 3, PM_APPLY = 4, PM_DOUBLE = 5, PM_NMODES = 6 };
+enum : int {
+    PM_SANDWICH = 0,
+    PM_FFT_FWD = 1,
+    PM_FFT_INV = 2,
+    PM_SPECRED = 3,
+    PM_APPLY = 4,
+    PM_DOUBLE = 5,
+    PM_ROUNDTRIP = 6,
+    PM_NMODES = 7
+};
 // |v|^2 w, Re(conj(partner) v) w, or (element-wise grid reductions only) Im(conj(partner) v) w
 enum : int { RK_ABS2 = 0, RK_BILIN = 1, RK_BILIN_IM = 2 };
 enum : int { WK_ONE = 0, WK_AXIS = 1, WK_GRID = 2 }; // weight 1, table[idx_axis], line-major table
@@ -349,12 +361,15 @@ __device__ __forceinline__ void finish_red(const RedDesc& rd, double* acc) {
 // Point-wise r-space factors on the E values a thread holds of one line: a full-grid table
 // (line-major: entry lbase + m), per-axis complex factors (the pass axis per element, the other
 // axes once per line), per-axis real factors and a scalar.
-template <typename R, int E, int T>
+// NAT: every table is indexed by the element's natural point index base + (m << log2S) instead of
+// the line-major lbase + m and the position m along the pass axis (the strided virtual axis of a
+// long 1-D axis, whose tables are in natural order).
+template <typename R, int E, int T, bool NAT = false>
 __device__ __forceinline__ void apply_factors(cplx_t<R>* v, int tid, long long base, long long lbase,
                                               const R* __restrict__ tr, const cplx_t<R>* __restrict__ tc,
                                               const cplx_t<R>* const* axc, const R* const* axr, int axis, int dim,
                                               const int* shift, const long long* nmask, const double* scale_dev,
-                                              uint32_t key) {
+                                              uint32_t key, int log2S = 0) {
     using V = cplx_t<R>;
     V lf = fone<V>();
     R lr = R(1);
@@ -373,11 +388,13 @@ __device__ __forceinline__ void apply_factors(cplx_t<R>* v, int tid, long long b
 #pragma unroll
         for (int u = 0; u < E; ++u) {
             const int m = tid + u * T;
+            const long long gi = NAT ? base + ((long long)m << log2S) : lbase + m;  // full-grid tables
+            const long long ai = NAT ? gi : (long long)m;                           // pass-axis tables
             V x = v[u];
-            if (tr) x = cscale(x, tr[lbase + m]);
-            if (tc) x = fmul(x, tc[lbase + m]);
-            if (pc) x = fmul(x, __ldg(pc + m));
-            if (pr) x = cscale(x, __ldg(pr + m));
+            if (tr) x = cscale(x, tr[gi]);
+            if (tc) x = fmul(x, tc[gi]);
+            if (pc) x = fmul(x, __ldg(pc + ai));
+            if (pr) x = cscale(x, __ldg(pr + ai));
             if (use_lf) x = fmul(x, lf);
             if (use_lr) x = cscale(x, lr);
             v[u] = x;
@@ -393,12 +410,14 @@ __device__ __forceinline__ void apply_factors(cplx_t<R>* v, int tid, long long b
 #pragma unroll
             for (int u = 0; u < E; ++u) {
                 const int m = tid + u * T;
+                const long long gi = NAT ? base + ((long long)m << log2S) : lbase + m;
+                const long long ai = NAT ? gi : (long long)m;
                 V x = v[u];
-                if (tr) x = cscale(x, tr[lbase + m]);
-                if (tc) x = fmul(x, tc[lbase + m]);
-                if (pc) x = (u == E / 2 - 1 || u == E / 2) ? fmul_dither(x, __ldg(pc + m), mix32(key + uint32_t(m)))
-                                                          : fmul(x, __ldg(pc + m));
-                if (pr) x = cscale(x, __ldg(pr + m));
+                if (tr) x = cscale(x, tr[gi]);
+                if (tc) x = fmul(x, tc[gi]);
+                if (pc) x = (u == E / 2 - 1 || u == E / 2) ? fmul_dither(x, __ldg(pc + ai), mix32(key + uint32_t(m)))
+                                                          : fmul(x, __ldg(pc + ai));
+                if (pr) x = cscale(x, __ldg(pr + ai));
                 x = fmul_dither(x, lf, mix32((key ^ 0x85ebca6bu) + uint32_t(m)));
                 if (use_lr) x = cscale(x, lr);
                 v[u] = x;
@@ -407,12 +426,14 @@ __device__ __forceinline__ void apply_factors(cplx_t<R>* v, int tid, long long b
 #pragma unroll
             for (int u = 0; u < E; ++u) {
                 const int m = tid + u * T;
+                const long long gi = NAT ? base + ((long long)m << log2S) : lbase + m;
+                const long long ai = NAT ? gi : (long long)m;
                 V x = v[u];
-                if (tr) x = cscale(x, tr[lbase + m]);
-                if (tc) x = fmul(x, tc[lbase + m]);
-                if (pc) x = (u == E / 2 - 1 || u == E / 2) ? fmul_dither(x, __ldg(pc + m), mix32(key + uint32_t(m)))
-                                                          : fmul(x, __ldg(pc + m));
-                if (pr) x = cscale(x, __ldg(pr + m));
+                if (tr) x = cscale(x, tr[gi]);
+                if (tc) x = fmul(x, tc[gi]);
+                if (pc) x = (u == E / 2 - 1 || u == E / 2) ? fmul_dither(x, __ldg(pc + ai), mix32(key + uint32_t(m)))
+                                                          : fmul(x, __ldg(pc + ai));
+                if (pr) x = cscale(x, __ldg(pr + ai));
                 if (use_lf) x = fmul(x, lf);
                 if (use_lr) x = cscale(x, lr);
                 v[u] = x;
@@ -534,7 +555,7 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
 #pragma unroll
     for (int k = 0; k < MAX_RED; ++k) acc[k] = 0.0;
 
-    if constexpr (MODE == PM_FFT_INV) {
+    if constexpr (MODE == PM_FFT_INV || MODE == PM_ROUNDTRIP) {
         fft_line_stages<L, E, +1, 0, TWS>(v, tid, line, tw, lsync);
     } else {
         fft_line_stages<L, E, -1, 0, TWS>(v, tid, line, tw, lsync);
@@ -544,6 +565,14 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
     if constexpr (MODE == PM_FFT_FWD || MODE == PM_FFT_INV) {
 #pragma unroll
         for (int u = 0; u < E; ++u) v[u] = cscale(v[u], a.scale);
+        store_out = true;
+    } else if constexpr (MODE == PM_ROUNDTRIP) {
+#pragma unroll
+        for (int u = 0; u < E; ++u) v[u] = cscale(v[u], a.scale);
+        if (active)
+            apply_factors<R, E, T, true>(v, tid, base, lbase, a.mid_real, a.mid_cplx, a.mid_ax_cplx, a.mid_ax_real,
+                                         a.axis, a.dim, a.shift, a.nmask, nullptr, key0 ^ 0x2545f491u, log2S);
+        fft_line_stages<L, E, -1, 0, TWS>(v, tid, line, tw, lsync);
         store_out = true;
     } else if constexpr (MODE == PM_SPECRED) {
         if (active) accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);

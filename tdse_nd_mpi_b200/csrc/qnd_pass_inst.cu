@@ -20,6 +20,7 @@ template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int m
     case PM_SPECRED: fn = QND_PICK(PM_SPECRED); break;
     case PM_APPLY: fn = QND_PICK(PM_APPLY); break;
     case PM_DOUBLE: fn = QND_PICK(PM_DOUBLE); break;
+    case PM_ROUNDTRIP: fn = QND_PICK(PM_ROUNDTRIP); break;
     default: fn = nullptr;
     }
 #undef QND_PICK
