@@ -38,6 +38,7 @@ extern "C" {
 #define QND_ENOMEM 3       /* device allocation failed */
 #define QND_ENORM 4        /* Gram-Schmidt norm below 1e-12 (QuantumND_imag.c:297-304) */
 #define QND_EUNSUPPORTED 5 /* configuration outside what this build implements */
+#define QND_ENONFINITE 6   /* QND_CHECK_FINITE=1: the state holds NaN or Inf after a run */
 
 #define QND_FP64 0  /* complex128 state, FP64 everywhere */
 #define QND_MIXED 1 /* complex64 state, FFT and phases in FP32, all reductions in FP64 */

@@ -12,7 +12,7 @@ import os
 PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG, "libqnd_b200.so")
 
-QND_OK, QND_EINVAL, QND_ECUDA, QND_ENOMEM, QND_ENORM, QND_EUNSUPPORTED = 0, 1, 2, 3, 4, 5
+QND_OK, QND_EINVAL, QND_ECUDA, QND_ENOMEM, QND_ENORM, QND_EUNSUPPORTED, QND_ENONFINITE = 0, 1, 2, 3, 4, 5, 6
 QND_FP64, QND_MIXED = 0, 1
 
 # (name, argtypes) for every symbol declared in include/qnd.h

@@ -172,6 +172,7 @@ struct qnd_ctx {
     DevBuf field_out, embed_src;                // qnd_field_samples host-output staging; qnd_state_embed source
     DevBuf err_flag;                            // set by a kernel whose bounded wait ran out
     DevBuf tune_buf;                            // scratch state of the staging autotuner
+    DevBuf finite_slot;                         // QND_CHECK_FINITE: the non-finite count
     std::map<std::tuple<const void*, int, int>, CUtensorMap> tmaps;  // strided-pass TMA views of states
 
     // A 1-D axis longer than one pass handles: N = n1 n2 (n1 >= 16, n2 <= 4096) as a virtual
@@ -814,6 +815,29 @@ static void grid_reduce(qnd_ctx* c, const void* psi, const RedDesc& rd_in, const
     }
     c->kernels_launched++;
     QND_CK(cudaGetLastError());
+}
+
+// Debug scan (QND_CHECK_FINITE=1): the count of state elements with a NaN or Inf part, read back
+// after the call's work; QND_ENONFINITE names the call when there are any.
+static void check_finite(qnd_ctx* c, const void* psi, const char* what) {
+    const char* e = std::getenv("QND_CHECK_FINITE");
+    if (!e || !std::atoi(e)) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    QND_CK(cudaStreamIsCapturing(c->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return;  // no read-back inside a capture
+    c->finite_slot.ensure(sizeof(double));
+    double* slot = c->finite_slot.as<double>();
+    RedDesc rd{};
+    rd.n = 1;
+    rd.kind[0] = RK_NONFINITE;
+    rd.wkind[0] = WK_ONE;
+    rd.scale[0] = 1.0;
+    rd.out = slot;
+    grid_reduce(c, psi, rd);
+    double bad = 0.0;
+    QND_CK(cudaMemcpyAsync(&bad, slot, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    QND_CK(cudaStreamSynchronize(c->stream));
+    if (bad > 0.0) QND_FAIL(QND_ENONFINITE, "%s: %.0f state elements hold NaN or Inf", what, bad);
 }
 
 // Axes in pass order: the contiguous axis first, axis 0 last (the last pass carries the epilogue).
@@ -2458,6 +2482,7 @@ int qnd_step_imag(qnd_ctx* ctx, void* psi_dev, int64_t nsteps) {
     set_device(ctx);
     imag_steps(ctx, psi_dev, nsteps, nullptr);
     QND_CK(cudaGetLastError());
+    check_finite(ctx, psi_dev, "qnd_step_imag");
     QND_API_END
 }
 
@@ -2495,6 +2520,7 @@ int qnd_step_length(qnd_ctx* ctx, void* psi_p_dev, const double* E_host, int64_t
     }
     unitary_fft(ctx, psi_p_dev, true);
     QND_CK(cudaGetLastError());
+    check_finite(ctx, psi_p_dev, "qnd_step_length");
     QND_API_END
 }
 
@@ -2512,6 +2538,7 @@ int qnd_step_velocity(qnd_ctx* ctx, void* psi_dev, const double* A_host, int64_t
         velocity_steps(ctx, psi_dev, 0, ch, nullptr, false);
     }
     QND_CK(cudaGetLastError());
+    check_finite(ctx, psi_dev, "qnd_step_velocity");
     QND_API_END
 }
 
@@ -2528,6 +2555,7 @@ int qnd_run_length(qnd_ctx* ctx, void* psi_r_dev, const double* E_host, int64_t 
     parse_obs(ctx, nobs, names, &nv);
     if (nv > 0) QND_NEED(obs_host);
     run_realtime(ctx, psi_r_dev, E_host, nullptr, nsteps, nobs, names, obs_host, false);
+    check_finite(ctx, psi_r_dev, "qnd_run_length");
     QND_API_END
 }
 
@@ -2547,6 +2575,7 @@ int qnd_run_velocity(qnd_ctx* ctx, void* psi_r_dev, const double* A_host, const 
         QND_NEED(alpha_host);
     }
     run_realtime(ctx, psi_r_dev, A_host, alpha_host, nsteps, nobs, names, obs_host, true);
+    check_finite(ctx, psi_r_dev, "qnd_run_velocity");
     QND_API_END
 }
 
@@ -2598,6 +2627,7 @@ int qnd_imag_propagate(qnd_ctx* ctx, void* const* states_dev, int j, int64_t nst
     }
     scale_state(ctx, states_dev[j], pending);
     check_gs_flag(ctx, j);
+    check_finite(ctx, states_dev[j], "qnd_imag_propagate");
     QND_API_END
 }
 
@@ -2654,6 +2684,7 @@ int qnd_run_length_dev(qnd_ctx* ctx, void* psi_r_dev, const double* E_dev, int64
         }
     }
     QND_CK(cudaGetLastError());
+    check_finite(ctx, psi_r_dev, "qnd_run_length_dev");
     QND_API_END
 }
 

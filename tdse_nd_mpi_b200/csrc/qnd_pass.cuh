@@ -50,8 +50,9 @@ enum : int {
     PM_ROUNDTRIP = 6,
     PM_NMODES = 7
 };
-// |v|^2 w, Re(conj(partner) v) w, or (element-wise grid reductions only) Im(conj(partner) v) w
-enum : int { RK_ABS2 = 0, RK_BILIN = 1, RK_BILIN_IM = 2 };
+// |v|^2 w, Re(conj(partner) v) w, or (element-wise grid reductions only) Im(conj(partner) v) w and
+// the count of elements with a non-finite part
+enum : int { RK_ABS2 = 0, RK_BILIN = 1, RK_BILIN_IM = 2, RK_NONFINITE = 3 };
 enum : int { WK_ONE = 0, WK_AXIS = 1, WK_GRID = 2 }; // weight 1, table[idx_axis], line-major table
 
 struct RedDesc {
@@ -236,6 +237,8 @@ __device__ __forceinline__ void accumulate_red(const RedDesc& rd, double* acc, V
         } else if (rd.kind[k] == RK_BILIN) {
             V p = partner[flat];
             val = double(p.x) * double(v.x) + double(p.y) * double(v.y);
+        } else if (rd.kind[k] == RK_NONFINITE) {
+            val = (isfinite(double(v.x)) && isfinite(double(v.y))) ? 0.0 : 1.0;
         } else {
             V p = partner[flat];
             val = double(p.x) * double(v.y) - double(p.y) * double(v.x);

@@ -4,7 +4,8 @@
   request's size, and the context works again once allocations succeed;
 * a zero initial state in imaginary time: the Gram-Schmidt norm collapse (QuantumND_imag.c:297-304)
   as QND_ENORM;
-* a truncated OUTPUT_IMAG: the real-time driver stops with the reference's read error and exit 1.
+* a truncated OUTPUT_IMAG: the real-time driver stops with the reference's read error and exit 1;
+* a NaN in the input state under the debug scan (QND_CHECK_FINITE=1): QND_ENONFINITE.
 """
 import os
 import subprocess
@@ -63,3 +64,25 @@ def test_truncated_output_imag_stops_the_real_driver(qnd_lib, tmp_path):
     r = subprocess.run([exe, "params.real"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
     assert r.returncode == 1
     assert "MPI Read Error during chunking" in r.stdout + r.stderr
+
+
+def test_nonfinite_state_is_reported_when_checking(qnd_lib, monkeypatch):
+    """QND_CHECK_FINITE=1 (the debug scan): a NaN planted in the host input makes the stepping call
+    return QND_ENONFINITE; a clean state passes; without the switch nothing is checked."""
+    from tdse_nd_mpi_b200 import Grid, QndError
+
+    shape, dr = (64, 64), (0.3, 0.3)
+    grid = Grid(2, shape, dr, "BM4", 0.05)
+    grid.set_potential("H_2D")
+    clean = O.smooth_state(shape, dr, 3)
+    bad = clean.copy()
+    bad[10, 20] = complex(np.nan, 0.0)
+    E = np.zeros((2, grid.s, 2))
+    grid.run_length(grid.state(bad), E, ["norm"])   # unchecked: NaN propagates silently
+    monkeypatch.setenv("QND_CHECK_FINITE", "1")
+    grid.run_length(grid.state(clean), E, ["norm"])
+    with pytest.raises(QndError) as ei:
+        grid.run_length(grid.state(bad), E, ["norm"])
+    assert ei.value.code == 6 and "NaN or Inf" in str(ei.value)
+    with pytest.raises(QndError):
+        grid.integration_step_imag(grid.state(bad), 1)
