@@ -691,6 +691,7 @@ static int staging_choice(qnd_ctx* c, const PassSpec& ps, int L, int log2S) {
         c->kernels_launched = k0;
         choice = ms[1] < 0.98f * ms[0] ? 1 : 0;
     }
+    c->tune_buf.reset();  // a one-time measurement: give the scratch state back
     std::lock_guard<std::mutex> lk(g_staging_mu);
     g_staging[key] = choice;
     return choice;
