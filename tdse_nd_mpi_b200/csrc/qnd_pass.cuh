@@ -480,12 +480,11 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
         tw = tw_s;
     }
 
-    pdl_wait();
-    pdl_launch_dependents();
-
     if constexpr (MODE == PM_DOUBLE || MODE == PM_SANDWICH) {
-        // tables needed after the first transforms: start their journey to L2 now
+        // the read-only tables: start their journey to L2 now, before the wait for the previous
+        // pass (which writes only the state), so that it overlaps that pass's tail
         if (active) {
+            if (a.pro_cplx) prefetch_row_l2<L, T>(a.pro_cplx + lbase, tid);
             if (a.mid_cplx) prefetch_row_l2<L, T>(a.mid_cplx + lbase, tid);
             if (a.mid_real) prefetch_row_l2<L, T>(a.mid_real + lbase, tid);
             if (a.epi_cplx) prefetch_row_l2<L, T>(a.epi_cplx + lbase, tid);
@@ -494,6 +493,9 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
                 if (a.red.wkind[k] == WK_GRID) prefetch_row_l2<L, T>(a.red.wtab[k] + lbase, tid);
         }
     }
+
+    pdl_wait();
+    pdl_launch_dependents();
 
     V v[E];
     if constexpr (STRIDED) {
