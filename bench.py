@@ -503,6 +503,68 @@ def ne2d_leg(torch, steps, imag_steps):
     return out
 
 
+def adjoint_leg(torch, steps, n_fd=4):
+    """The H_3D adjoint configuration: 256^3, DR 0.3, dt 0.05, BM4, V = -1/sqrt(r^2 + 0.5), an 800 nm
+    field sampled at the sub-step times with seeded 1e-3 relative perturbations, J = the norm beyond
+    |r| > 25 a.u., checkpoints every 50 steps. Times the forward run (qnd_run_length) and the adjoint
+    call (J and dJ/dE for every sample, qnd_adjoint_length) with CUDA events, and checks the gradient
+    at n_fd seeded samples against central differences of the forward J."""
+    from tdse_nd_mpi_b200 import Grid
+    from tdse_nd_mpi_b200.adjoint import absorbed_weight
+
+    n, dr, dt = 256, 0.3, 0.05
+    g = Grid(3, (n, n, n), (dr, dr, dr), "BM4", dt)
+    x = g.axis_r(0)
+    X = np.meshgrid(x, x, x, indexing="ij")
+    r = np.sqrt(X[0] ** 2 + X[1] ** 2 + X[2] ** 2)
+    g.set_potential(-1.0 / np.sqrt(r * r + 0.5))
+    g.set_cap(0.05, 5.0)
+    w = absorbed_weight(g, 25.0)
+    psi0 = (np.exp(-(r ** 2) / 2) * np.exp(1j * 1.5 * X[0])).astype(np.complex128)
+    psi0 /= np.sqrt(np.sum(np.abs(psi0) ** 2) * dr ** 3)
+    del X, r
+    rng = np.random.default_rng(5)
+    w800 = 45.5637639947958 / 800.0
+    t = np.arange(steps)[:, None] * dt + np.cumsum(np.r_[g.as_scaled[0], g.as_scaled[1:-1:2] + g.as_scaled[2::2]])
+    E = np.zeros((steps, g.s, 3))
+    E[:, :, 0] = 0.0533803 * np.sin(w800 * t) * np.sin(np.pi * t / (steps * dt)) ** 2 * (
+        1.0 + 1e-3 * rng.standard_normal((steps, g.s)))
+    st, work = g.state(psi0), g.state()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def forward(Ep):
+        work.upload(psi0)
+        g.run_length(work, Ep, [])
+        return g.dNr * float(np.sum(w * np.abs(work.download()) ** 2))
+
+    forward(E[:50])  # warm-up: tables, chunk graphs, staging measurement
+    torch.cuda.synchronize()
+    a.record()
+    J_fwd = forward(E)
+    b.record()
+    torch.cuda.synchronize()
+    fwd_ms = a.elapsed_time(b)
+    a.record()
+    J, grad = g.adjoint_length(st, E, w, checkpoint=50)
+    b.record()
+    torch.cuda.synchronize()
+    adj_ms = a.elapsed_time(b)
+    eps, checks = 1e-5, []
+    for _ in range(n_fd):
+        idx = (int(rng.integers(steps // 4, steps)), int(rng.integers(0, g.s)), 0)
+        Ep, Em = E.copy(), E.copy()
+        Ep[idx] += eps
+        Em[idx] -= eps
+        fd = (forward(Ep) - forward(Em)) / (2 * eps)
+        checks.append({"sample": list(idx), "adjoint": float(grad[idx]), "central_difference": fd,
+                       "rel_diff": abs(fd - float(grad[idx])) / max(abs(fd), 1e-300)})
+    return {"grid": [n, n, n], "steps": steps, "checkpoint": 50, "J": J, "J_forward": J_fwd,
+            "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "adjoint_over_forward": adj_ms / fwd_ms,
+            "gradient_entries": int(grad.size), "fd_checks": checks,
+            "what": "CUDA events around whole calls; the adjoint call runs the forward pass, the "
+                    "checkpointed recomputation and the backward sweep"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -513,6 +575,8 @@ def main():
     ap.add_argument("--imag-steps", type=int, default=100, help="imaginary-time steps for the initial state")
     ap.add_argument("--sweep", type=int, default=0, metavar="STEPS",
                     help="also time the 96-member sweep configuration for STEPS steps (key 'sweep')")
+    ap.add_argument("--adjoint", type=int, default=0, metavar="STEPS",
+                    help="also run the H_3D 256^3 adjoint configuration for STEPS steps (key 'adjoint')")
     ap.add_argument("--ne2d", type=int, default=0, metavar="STEPS",
                     help="also run the Ne_2D-style 2048^2 BM6 configuration: 8 imaginary-time states, then "
                          "STEPS real-time steps in FP64 and mixed precision (key 'ne2d')")
@@ -695,6 +759,8 @@ def main():
         line["sweep"] = sweep_leg(torch, args.sweep)
     if args.ne2d > 0 and world == 1:
         line["ne2d"] = ne2d_leg(torch, args.ne2d, max(20, args.imag_steps))
+    if args.adjoint > 0 and world == 1:
+        line["adjoint"] = adjoint_leg(torch, args.adjoint)
     if rank == 0:
         print(json.dumps(line), flush=True)
     grid.close()
