@@ -576,18 +576,15 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 static EncodeTiledFn tensor_map_encoder() {
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    static const EncodeTiledFn fn = []() -> EncodeTiledFn {  // looked up once, thread-safe
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q{};
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-        else
-            cudaGetLastError();
-    }
+            return reinterpret_cast<EncodeTiledFn>(p);
+        cudaGetLastError();
+        return nullptr;
+    }();
     return fn;
 }
 
@@ -721,15 +718,19 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     const long long nlines = c->n / L;
     const long long ngroups = (nlines + info.G - 1) / info.G;
     const int staging = !strided ? 0 : ps.force_staging >= 0 ? ps.force_staging : staging_choice(c, ps, L, log2S);
-    static std::map<std::pair<const void*, int>, LaunchCfg> configured;  // per (kernel, device)
-    auto cfg_key = std::make_pair(info.fn, c->device);
-    auto cfg_it = configured.find(cfg_key);
-    if (cfg_it == configured.end()) {
-        QND_CK(cudaFuncSetAttribute(info.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(info.smem)));
-        LaunchCfg cfg;
-        QND_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cfg.blocks_per_sm, info.fn, info.nt, info.smem));
-        if (cfg.blocks_per_sm < 1) QND_FAIL(QND_ECUDA, "pass kernel for L=%d does not fit on an SM", L);
-        cfg_it = configured.emplace(cfg_key, cfg).first;
+    // per (kernel, device), shared by the contexts of every host thread
+    static std::map<std::pair<const void*, int>, LaunchCfg> configured;
+    static std::mutex configured_mu;
+    {
+        std::lock_guard<std::mutex> lk(configured_mu);
+        auto cfg_key = std::make_pair(info.fn, c->device);
+        if (configured.find(cfg_key) == configured.end()) {
+            QND_CK(cudaFuncSetAttribute(info.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(info.smem)));
+            LaunchCfg cfg;
+            QND_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cfg.blocks_per_sm, info.fn, info.nt, info.smem));
+            if (cfg.blocks_per_sm < 1) QND_FAIL(QND_ECUDA, "pass kernel for L=%d does not fit on an SM", L);
+            configured.emplace(cfg_key, cfg);
+        }
     }
     const long long blocks = std::max<long long>(1, ngroups);
     RedDesc red = ps.red;

@@ -119,3 +119,28 @@ def test_one_graph_sweep_matches_members_alone(qnd_lib, precision, monkeypatch):
     for a, b in zip(together, direct):
         np.testing.assert_array_equal(a["obs"], b["obs"])
         np.testing.assert_array_equal(a["psi"], b["psi"])
+
+
+@pytest.mark.gpu
+def test_contexts_on_several_host_threads_match_one_thread(qnd_lib):
+    """Different contexts driven from different host threads at once (the C calls release the
+    interpreter lock, so they overlap): the same results as one thread running them in turn."""
+    import threading
+
+    from tdse_nd_mpi_b200.batch import run_members
+
+    members = [_member((128, 128), 21), _member((256,), 22, "Verlet"), _member((64, 64, 32), 23), _member((8192,), 24)]
+    alone = run_members(members)
+    got = [None] * len(members)
+
+    def work(i):
+        got[i] = run_members([members[i]])[0]
+
+    threads = [threading.Thread(target=work, args=(i,)) for i in range(len(members))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=300)
+    for a, b in zip(alone, got):
+        np.testing.assert_array_equal(a["obs"], b["obs"])
+        np.testing.assert_array_equal(a["psi"], b["psi"])
