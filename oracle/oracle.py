@@ -116,7 +116,7 @@ def ref_lib(fast: bool = False):
     if key not in _lib_ref:
         path = REF_FAST_SO if fast else REF_SO
         if not os.path.exists(path):
-            raise FileNotFoundError(f"{path} not built (needs the reference sources: make -C oracle ref)")
+            raise FileNotFoundError(f"{path} not built (needs the reference sources: make -C oracle ref REF=<reference root>)")
         L = C.CDLL(path)
         L.ref_create.restype = _vp
         L.ref_create.argtypes = [C.c_int, C.POINTER(_ll), _dp, C.c_char_p, C.c_double, C.c_double, C.c_char_p,

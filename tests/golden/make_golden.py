@@ -1,6 +1,6 @@
 """Generate the golden vectors in tests/golden/ from the reference's OWN sources.
 
-Runs the unmodified QuantumND C sources (compiled by ``make -C oracle ref`` against
+Runs the unmodified QuantumND C sources (compiled by ``make -C oracle ref REF=<reference root>`` against
 the single-rank MPI / FFTW-API shims) on seeded inputs and stores inputs and
 outputs as compressed .npz fixtures. The reference is only available where its
 sources are (this script is not run by tests); the fixtures are committed so
@@ -130,7 +130,7 @@ def fft_fixture():
 
 if __name__ == "__main__":
     if not O.ref_available():
-        sys.exit("oracle/_ref/libqnd_ref.so missing: run `make -C oracle ref` where the reference sources exist")
+        sys.exit("oracle/_ref/libqnd_ref.so missing: run `make -C oracle ref REF=<reference root>` where the reference sources exist")
     steps_fixture()
     observables_fixture()
     trajectory_fixture()
