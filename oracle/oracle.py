@@ -141,6 +141,7 @@ def ref_lib(fast: bool = False):
         L.ref_observables.argtypes = [_vp, _vp, C.c_int, C.POINTER(C.c_char_p), _dp, _dp]
         L.ref_run_length.argtypes = [_vp, _vp, _dp, _ll, C.c_int, C.POINTER(C.c_char_p), _dp]
         L.ref_run_velocity.argtypes = [_vp, _vp, _dp, _dp, _ll, C.c_int, C.POINTER(C.c_char_p), _dp]
+        L.ref_run_length_ext.argtypes = [_vp, _vp, _dp, _ll, C.c_int, C.POINTER(C.c_char_p), C.POINTER(_dp), _dp]
         L.ref_to_p.argtypes = [_vp, _vp]
         L.ref_final_observables.argtypes = [_vp, _vp, C.c_double, C.c_double, _dp, C.c_double, C.c_int, C.c_int,
                                             C.POINTER(C.c_char_p)]
@@ -441,6 +442,19 @@ class RefCtx(_Base):
         out = np.zeros((nsteps, max(1, nv)))
         self.L.ref_run_length(self.h, _ptr(self._check(psi_r)), _dptr(E), nsteps, len(names), _cstrs(names),
                               _dptr(out))
+        return out[:, :nv]
+
+    def run_length_ext(self, psi_r, E, names, gradv=None):
+        """ref_run_length with the "norm" and "accel" extensions computed on the same states
+        (gradv: dim arrays dV/dx_j in natural order, needed for "accel")."""
+        E = _f64(E)
+        nsteps = E.shape[0]
+        nv = sum(obs_width(n, self.dim) for n in names)
+        out = np.zeros((nsteps, max(1, nv)))
+        gv = [_f64(g) for g in gradv] if gradv is not None else []
+        arr = (C.POINTER(C.c_double) * max(1, self.dim))(*[_dptr(g) for g in gv]) if gv else None
+        self.L.ref_run_length_ext(self.h, _ptr(self._check(psi_r)), _dptr(E), nsteps, len(names), _cstrs(names),
+                                  arr, _dptr(out))
         return out[:, :nv]
 
     def run_velocity(self, psi_r, A, alpha_steps, names):

@@ -182,6 +182,86 @@ int ref_run_length(RefCtx *c, double complex *psi, const double *E, long long ns
 }
 
 /*
+ * The loop of ref_run_length with the two observable extensions of this project (the reference
+ * has neither) evaluated on the same r-space state at the same point of each step:
+ *   "norm"  = sum |psi|^2 dNr                        (1 value)
+ *   "accel" = -sum |psi|^2 dV/dx_j dNr, j < dim       (dim values; gradv[j] in natural order)
+ * Every other name goes to the reference's own Calculation_global_observables. Output columns
+ * follow the order of names. Used for the CPU baseline, where both sides must compute the same
+ * observables of the same run.
+ */
+int ref_run_length_ext(RefCtx *c, double complex *psi, const double *E, long long nsteps, int nobs, char **names,
+                       const double *const *gradv, double *obs_out) {
+    MeshGrid *g = &c->grid;
+    ptrdiff_t n = g->dim_HS;
+    int dim = c->P.dim, sd = c->Int.s_integrator * dim;
+    double alpha[8] = {0};
+    char *rnames[32];
+    int nref = 0, width = 0, kind[32], wref[32];
+    for (int k = 0; k < nobs && k < 32; ++k) {
+        if (strcmp(names[k], "norm") == 0) {
+            kind[k] = 1;
+            width += 1;
+        } else if (strcmp(names[k], "accel") == 0) {
+            kind[k] = 2;
+            width += dim;
+        } else {
+            kind[k] = 0;
+            rnames[nref++] = names[k];
+        }
+    }
+    Observables Obs;
+    memset(&Obs, 0, sizeof Obs);
+    Initialize_observables(&Obs, rnames, nref, dim, MPI_COMM_WORLD);
+    for (int k = 0, q = 0; k < nobs && k < 32; ++k)
+        if (kind[k] == 0) wref[k] = Obs.dimensions[q++];
+    width += Obs.total_values;
+    for (ptrdiff_t i = 0; i < n; i++) g->in[i] = psi[i];
+    fftw_execute(g->plan_forward);
+    for (ptrdiff_t i = 0; i < n; i++) psi[i] = g->out[i] * sqrt(g->fft_scaling);
+    for (long long it = 0; it < nsteps; ++it) {
+        if (width > 0) {
+            for (ptrdiff_t i = 0; i < n; i++) g->in[i] = psi[i];
+            fftw_execute(g->plan_backward);
+            for (ptrdiff_t i = 0; i < n; i++) psi[i] = g->out[i] * sqrt(g->fft_scaling);
+            for (int j = 0; j < dim; j++) alpha[j] = 0.;
+            if (Obs.total_values > 0) Calculation_global_observables(psi, dim, g, &Obs, alpha, MPI_COMM_WORLD);
+            double nrm = 0.0, acc[8] = {0};
+#pragma omp parallel for reduction(+ : nrm)
+            for (ptrdiff_t i = 0; i < n; i++) nrm += creal(psi[i] * conj(psi[i]));
+            for (int j = 0; j < dim && gradv; j++) {
+                double a = 0.0;
+                const double *gv = gradv[j];
+                if (!gv) continue;
+#pragma omp parallel for reduction(+ : a)
+                for (ptrdiff_t i = 0; i < n; i++) a += creal(psi[i] * conj(psi[i])) * gv[i];
+                acc[j] = -a * g->dNr;
+            }
+            double *row = obs_out + it * width;
+            for (int k = 0, col = 0, off = 0; k < nobs && k < 32; ++k) {
+                if (kind[k] == 1) {
+                    row[col++] = nrm * g->dNr;
+                } else if (kind[k] == 2) {
+                    for (int j = 0; j < dim; j++) row[col++] = acc[j];
+                } else {
+                    for (int j = 0; j < wref[k]; j++) row[col++] = Obs.values[off + j];
+                    off += wref[k];
+                }
+            }
+            for (ptrdiff_t i = 0; i < n; i++) g->in[i] = psi[i];
+            fftw_execute(g->plan_forward);
+            for (ptrdiff_t i = 0; i < n; i++) psi[i] = g->out[i] * sqrt(g->fft_scaling);
+        }
+        Integration_step_length(psi, E + it * sd, dim, g, &c->Int);
+    }
+    for (ptrdiff_t i = 0; i < n; i++) g->in[i] = psi[i];
+    fftw_execute(g->plan_backward);
+    for (ptrdiff_t i = 0; i < n; i++) psi[i] = g->out[i] * sqrt(g->fft_scaling);
+    Finalize_observables(&Obs);
+    return width;
+}
+
+/*
  * Velocity-gauge loop as QuantumND_real.c:168-187. alpha_steps[it*dim..] is
  * A(t_it) for the observables (Field_vectors at P.time[itime]); A holds the
  * sub-step samples [nsteps][s][dim].

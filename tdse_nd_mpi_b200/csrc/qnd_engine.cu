@@ -527,6 +527,16 @@ static void ensure_red_scratch(qnd_ctx* c, long long blocks) {
     }
 }
 
+// Tries of the bounded wait of a strided pass for its TMA box loads (2^20). QND_TMA_WAIT_TRIES
+// overrides it, read at every launch: a host-side way to make the wait run out (0 tries) and check
+// that path (the CTAs then leave the state untouched and the next synchronising call reports it).
+static int tma_wait_tries() {
+    const char* e = std::getenv("QND_TMA_WAIT_TRIES");
+    if (!e || !*e) return 1 << 20;
+    const long v = std::strtol(e, nullptr, 10);
+    return v < 0 ? 0 : (v > (1 << 20) ? (1 << 20) : int(v));
+}
+
 template <typename R> static void fill_args(qnd_ctx* c, const PassSpec& ps, PassArgs<R>& a) {
     using V = cplx_t<R>;
     std::memset(&a, 0, sizeof a);
@@ -565,6 +575,7 @@ template <typename R> static void fill_args(qnd_ctx* c, const PassSpec& ps, Pass
     a.seed = uint32_t(c->kernels_launched) * 0x9e3779b9u + 0x632be5abu;
     a.red = ps.red;
     a.err = c->err_flag.as<int>();
+    a.tma_wait_tries = tma_wait_tries();
 }
 
 struct LaunchCfg {
@@ -702,7 +713,8 @@ static void check_device_error(qnd_ctx* c) {
     QND_CK(cudaStreamSynchronize(c->stream));
     if (flag) {
         QND_CK(cudaMemsetAsync(c->err_flag.p, 0, sizeof(int), c->stream));
-        QND_FAIL(QND_ECUDA, "a pass kernel's wait for its TMA box loads ran out (results of that call are invalid)");
+        QND_FAIL(QND_ECUDA, "a pass kernel's wait for its TMA box loads ran out; the CTAs concerned left their "
+                            "lines untransformed (results of that call are invalid)");
     }
 }
 
@@ -1738,7 +1750,7 @@ static void run_realtime(qnd_ctx* c, void* psi, const double* field_host, const 
         }
     }
     QND_CK(cudaGetLastError());
-    if (nv > 0) check_device_error(c);  // the rows were read back: the call synchronised anyway
+    check_device_error(c);  // a wait that ran out in this call is reported by this call
 }
 
 // ---------------------------------------------------------------- adjoint --

@@ -108,6 +108,7 @@ template <typename R> struct PassArgs {
     // those loads runs out
     int use_tma;
     int* err;
+    int tma_wait_tries;          // tries of the bounded wait for those loads before the CTA gives up
     CUtensorMap tmap;
 };
 
@@ -503,11 +504,13 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
             // the CTA's G lines as L/BOXL boxes {G lines, BOXL rows} in [row][line] order, loaded by TMA
             // (the host enables this only when every group is full and the boxes meet the 16-byte rules)
             __shared__ __align__(8) uint64_t tma_bar;
+            __shared__ int tma_gave_up;
             constexpr int BOXL = L < 256 ? L : 256;
             const long long lam0 = g * G;
             if (t == 0) {
                 mbar_init(&tma_bar, 1);
                 mbar_init_fence();
+                tma_gave_up = 0;
             }
             __syncthreads();
             if (t == 0) {
@@ -517,9 +520,23 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
 #pragma unroll 1
                 for (int c = 0; c < L / BOXL; ++c) tma_load_3d(lines + c * BOXL * G, &a.tmap, x, c * BOXL, z, &tma_bar);
             }
-            if (!mbar_wait_bounded(&tma_bar, 0, 1 << 20)) {
-                if (tid == 0 && a.err) atomicExch(a.err, 1);
-                mbar_wait_bounded(&tma_bar, 0, 1 << 20);  // still give the copies in flight their time
+            if (!mbar_wait_bounded(&tma_bar, 0, a.tma_wait_tries)) tma_gave_up = 1;
+            __syncthreads();
+            if (tma_gave_up) {
+                // The CTA's lines did not arrive in time (one decision for the whole CTA). Give the
+                // copies in flight a second bounded wait so that none lands after the CTA has left,
+                // raise the error flag, and leave the state untouched: no transform, no store. The CTA
+                // still takes its ticket in the grid reduction (with nothing), so that the last CTA
+                // finishes it and resets the counter.
+                mbar_wait_bounded(&tma_bar, 0, 1 << 20);
+                if (t == 0 && a.err) atomicExch(a.err, 1);
+                if (MODE == PM_SPECRED || a.red.n) {
+                    double none[MAX_RED];
+#pragma unroll
+                    for (int k = 0; k < MAX_RED; ++k) none[k] = 0.0;
+                    finish_red<NT>(a.red, none);
+                }
+                return;
             }
 #pragma unroll
             for (int u = 0; u < E; ++u) v[u] = lines[(tid + u * T) * G + w];

@@ -5,8 +5,12 @@
 * a zero initial state in imaginary time: the Gram-Schmidt norm collapse (QuantumND_imag.c:297-304)
   as QND_ENORM;
 * a truncated OUTPUT_IMAG: the real-time driver stops with the reference's read error and exit 1;
-* a NaN in the input state under the debug scan (QND_CHECK_FINITE=1): QND_ENONFINITE.
+* a NaN in the input state under the debug scan (QND_CHECK_FINITE=1): QND_ENONFINITE;
+* the bounded wait of a strided pass for its TMA box loads running out (QND_TMA_WAIT_TRIES=0 makes
+  the first wait give up at once, while the second, draining wait keeps its full limit so that every
+  load lands before the CTA leaves): QND_ECUDA, and the CTAs concerned leave their lines untouched.
 """
+import sys
 import os
 import subprocess
 
@@ -86,3 +90,51 @@ def test_nonfinite_state_is_reported_when_checking(qnd_lib, monkeypatch):
     assert ei.value.code == 6 and "NaN or Inf" in str(ei.value)
     with pytest.raises(QndError):
         grid.integration_step_imag(grid.state(bad), 1)
+
+
+_TMA_SCRIPT = r"""
+import os, sys
+import numpy as np
+sys.path.insert(0, {root!r})
+from tdse_nd_mpi_b200 import Grid, QndError
+from oracle import oracle as O
+shape, dr = (1024, 1024), (0.2, 0.2)
+g = Grid(2, shape, dr, "BM4", 0.05)
+psi0 = O.smooth_state(shape, dr, 2)
+st = g.state(psi0)
+os.environ["QND_TMA_WAIT_TRIES"] = "0"
+g.to_p(st)                       # contiguous pass, then the strided pass (TMA boxes) that gives up
+try:
+    g.synchronize()
+    print("NO_ERROR")
+except QndError as e:
+    print("CODE", e.code, "ran out" in str(e))
+got = st.download()              # the flag was cleared by the report
+# only the contiguous axis was transformed: the strided CTAs stored nothing
+want = np.fft.fft(psi0, axis=1) / np.sqrt(1024.0)
+print("HALF_ERR", np.linalg.norm(got - want) / np.linalg.norm(want))
+del os.environ["QND_TMA_WAIT_TRIES"]
+st.upload(psi0)
+g.to_p(st)
+g.synchronize()
+want = np.fft.fft2(psi0) / 1024.0
+print("FULL_ERR", np.linalg.norm(st.download() - want) / np.linalg.norm(want))
+"""
+
+
+def test_tma_wait_that_runs_out_is_reported_and_leaves_the_lines(qnd_lib):
+    """QND_TMA_WAIT_TRIES=0 (a host-side setting, read at each launch): every strided CTA of a 1024^2
+    FP64 unitary transform gives up on its first wait, drains its loads with the second, raises the
+    error flag and stores nothing. The next synchronising call returns QND_ECUDA ("ran out"); the
+    state then holds the contiguous axis' transform alone; without the setting the same context
+    transforms correctly. Run in a child process with the staging fixed to TMA boxes (QND_TUNE=0:
+    1024-point strided lines use them), so that no staging measurement sees the setting."""
+    env = dict(os.environ, QND_TUNE="0")
+    env.pop("QND_NO_TMA", None)
+    r = subprocess.run([sys.executable, "-c", _TMA_SCRIPT.format(root=ROOT)], env=env, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = dict(line.split(" ", 1) for line in r.stdout.strip().splitlines())
+    assert out.get("CODE") == "2 True", r.stdout
+    assert float(out["HALF_ERR"]) < 1e-13, r.stdout
+    assert float(out["FULL_ERR"]) < 1e-13, r.stdout

@@ -191,3 +191,37 @@ def test_final_spectra_restatement_matches_reference(shape, dr, pot):
     np.testing.assert_allclose(pmd[:, 0], data[:, 0], rtol=0, atol=1e-13 * data[:, 0].max())
     live = data[:, 0] > 1e-10 * data[:, 0].max()
     assert np.max(np.abs(np.angle(np.exp(1j * (pmd[live, 1] - data[live, 1]))))) < 1e-9
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference not compiled here (needs its sources)")
+def test_reference_loop_with_extension_observables_matches_oracle():
+    """ref_run_length_ext (the reference's own length-gauge loop with norm and accel computed on the
+    same states, the CPU baseline's loop) against the oracle's run_length with the same observables,
+    a custom potential and a CAP: identical states, observables within summation-order rounding."""
+    dim, nr, dr = 2, (32, 64), (0.3, 0.25)
+    x = [-0.5 * n * d + np.arange(n) * d for n, d in zip(nr, dr)]
+    X, Y = np.meshgrid(*x, indexing="ij")
+    r2 = X * X + Y * Y
+    V = -1.0 / np.sqrt(r2 + 0.64)
+    grads = [X / (r2 + 0.64) ** 1.5, Y / (r2 + 0.64) ** 1.5]
+    vcap = 0.02 * (np.abs(X) > 3.5) + 0.01 * (np.abs(Y) > 6.0)
+    o = O.OracleCtx(dim, nr, dr, "BM4", 0.05, nthreads=2)
+    o.set_vpot(V)
+    o.set_vcap(vcap)
+    for j in range(dim):
+        o.set_gradv(j, grads[j])
+    r = O.RefCtx(dim, nr, dr, "BM4", 0.05, "H_2D", (0.0, 0.0), nthreads=2)
+    r.set_vpot(V)
+    r.set_vcap(vcap)
+    psi = O.seeded_state(nr, 4)
+    E = np.random.default_rng(9).standard_normal((4, o.s, dim)) * 0.05
+    names = ["norm", "dipole_r", "accel"]
+    a, b = psi.copy(), psi.copy()
+    got = r.run_length_ext(b, E, names, grads)
+    want = o.run_length(a, E, names)
+    assert got.shape == (4, 5)
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-14)
+    assert np.array_equal(a, b)
+    # the reference's own columns are the reference's values
+    c = psi.copy()
+    np.testing.assert_array_equal(got[:, 1:3], r.run_length(c, E, ["dipole_r"]))

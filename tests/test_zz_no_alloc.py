@@ -42,21 +42,27 @@ def _names(names):
     return arr
 
 
-@pytest.mark.parametrize("shape,dr,precision", [((1024, 1024), (0.2, 0.2), "fp64"),
-                                                ((256, 256), (0.2, 0.2), "mixed"),
-                                                ((16, 32, 64), (0.5, 0.4, 0.3), "fp64"),
-                                                ((4096,), (0.1,), "fp64")])
-def test_noalloc_matches_qnd_observables_two_calls(qnd_lib, shape, dr, precision):
+# More than 8 values (the accumulators of one reduction launch) in 3-D: the call splits them over
+# several launches that reuse the shared partial sums and ticket counter back to back.
+MANY = ["dipole_r", "accel", "norm", "dipole_r"]
+
+
+@pytest.mark.parametrize("shape,dr,precision,names", [((1024, 1024), (0.2, 0.2), "fp64", NAMES),
+                                                      ((256, 256), (0.2, 0.2), "mixed", NAMES),
+                                                      ((16, 32, 64), (0.5, 0.4, 0.3), "fp64", NAMES),
+                                                      ((4096,), (0.1,), "fp64", NAMES),
+                                                      ((32, 64, 128), (0.4, 0.3, 0.2), "fp64", MANY)])
+def test_noalloc_matches_qnd_observables_two_calls(qnd_lib, shape, dr, precision, names):
     import torch
 
     grid = _grid(shape, dr, precision)
     st = grid.state(O.smooth_state(shape, dr, 7))
-    ref = grid.observables(st, NAMES)          # the allocating entry point
+    ref = grid.observables(st, names)          # the allocating entry point
     nv = len(ref)
     out = torch.full((2, nv), float("nan"), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()                   # the fill runs on torch's stream, the reductions on the context's
     for call in range(2):
-        rc = qnd_lib.qnd_observables_rspace_noalloc(grid.h, C.c_void_p(st.ptr), len(NAMES), _names(NAMES),
+        rc = qnd_lib.qnd_observables_rspace_noalloc(grid.h, C.c_void_p(st.ptr), len(names), _names(names),
                                                     C.c_void_p(out[call].data_ptr()))
         assert rc == 0, qnd_lib.qnd_last_error()
     assert qnd_lib.qnd_synchronize(grid.h) == 0
