@@ -726,7 +726,12 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     const int log2S = ps.vL ? ps.vlog2S : c->shift[ax];
     const void* tw = ps.vL ? ps.vtw : c->tw[ax].p;
     const bool strided = log2S > 0;
-    const PassKernelInfo info = lookup_pass(c->fp64, L, strided, ps.mode);
+    // passes that reduce run the instantiation that carries the reduction code; the others keep its
+    // registers for the transform
+    int kmode = ps.mode;
+    if (ps.red.n && ps.mode == PM_SANDWICH) kmode = PM_SANDWICH_RED;
+    if (ps.red.n && ps.mode == PM_DOUBLE) kmode = PM_DOUBLE_RED;
+    const PassKernelInfo info = lookup_pass(c->fp64, L, strided, kmode);
     const long long nlines = c->n / L;
     const long long ngroups = (nlines + info.G - 1) / info.G;
     const int staging = !strided ? 0 : ps.force_staging >= 0 ? ps.force_staging : staging_choice(c, ps, L, log2S);

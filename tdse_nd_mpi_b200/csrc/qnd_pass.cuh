@@ -48,8 +48,18 @@ enum : int {
     PM_APPLY = 4,
     PM_DOUBLE = 5,
     PM_ROUNDTRIP = 6,
-    PM_NMODES = 7
+    PM_SANDWICH_RED = 7,  // PM_SANDWICH / PM_DOUBLE with fused reductions: separate instantiations, so that
+    PM_DOUBLE_RED = 8,    // the passes without reductions (most of a chain) keep their registers for the FFT
+    PM_NMODES = 9
 };
+// The transform structure of a mode (the reducing variants share their base mode's) and whether the
+// mode can carry reductions at all.
+__host__ __device__ constexpr int pass_base_mode(int m) {
+    return m == PM_SANDWICH_RED ? PM_SANDWICH : (m == PM_DOUBLE_RED ? PM_DOUBLE : m);
+}
+__host__ __device__ constexpr bool pass_mode_reduces(int m) {
+    return m == PM_SANDWICH_RED || m == PM_DOUBLE_RED || m == PM_SPECRED || m == PM_APPLY;
+}
 // |v|^2 w, Re(conj(partner) v) w, or (element-wise grid reductions only) Im(conj(partner) v) w and
 // the count of elements with a non-finite part
 enum : int { RK_ABS2 = 0, RK_BILIN = 1, RK_BILIN_IM = 2, RK_NONFINITE = 3 };
@@ -446,9 +456,11 @@ __device__ __forceinline__ void apply_factors(cplx_t<R>* v, int tid, long long b
     }
 }
 
-template <typename R, int L, bool STRIDED, int MODE>
+template <typename R, int L, bool STRIDED, int KMODE>
 __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
     qnd_pass_kernel(const __grid_constant__ PassArgs<R> a) {
+    constexpr int MODE = pass_base_mode(KMODE);
+    constexpr bool HAS_RED = pass_mode_reduces(KMODE);
     using V = cplx_t<R>;
     using SH = PassShape<R, L>;
     constexpr int E = SH::E, T = SH::T, G = SH::G, NT = SH::NT, LS = SH::LS;
@@ -490,8 +502,9 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
             if (a.mid_real) prefetch_row_l2<L, T>(a.mid_real + lbase, tid);
             if (a.epi_cplx) prefetch_row_l2<L, T>(a.epi_cplx + lbase, tid);
             if (a.epi_real) prefetch_row_l2<L, T>(a.epi_real + lbase, tid);
-            for (int k = 0; k < a.red.n; ++k)
-                if (a.red.wkind[k] == WK_GRID) prefetch_row_l2<L, T>(a.red.wtab[k] + lbase, tid);
+            if constexpr (HAS_RED)
+                for (int k = 0; k < a.red.n; ++k)
+                    if (a.red.wkind[k] == WK_GRID) prefetch_row_l2<L, T>(a.red.wtab[k] + lbase, tid);
         }
     }
 
@@ -530,7 +543,7 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
                 // finishes it and resets the counter.
                 mbar_wait_bounded(&tma_bar, 0, 1 << 20);
                 if (t == 0 && a.err) atomicExch(a.err, 1);
-                if (MODE == PM_SPECRED || a.red.n) {
+                if (HAS_RED && (MODE == PM_SPECRED || a.red.n)) {
                     double none[MAX_RED];
 #pragma unroll
                     for (int k = 0; k < MAX_RED; ++k) none[k] = 0.0;
@@ -613,11 +626,12 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
                 apply_factors<R, E, T>(v, tid, base, lbase, a.mid_real, a.mid_cplx, a.mid_ax_cplx, a.mid_ax_real,
                                        a.axis, a.dim, a.shift, a.nmask, nullptr, key0 ^ 0x2545f491u);
                 // a step boundary inside the pass: observables of the state between the two steps
-                if (a.red_at_mid && a.red.n)
+                if (HAS_RED && a.red_at_mid && a.red.n)
                     accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);
             }
             // finish those reductions here, so that no accumulator stays live through the second sandwich
-            if (a.red_at_mid && a.red.n) finish_red<NT>(a.red, acc);
+            if constexpr (HAS_RED)
+                if (a.red_at_mid && a.red.n) finish_red<NT>(a.red, acc);
             fft_line_stages<L, E, -1, 0, TWS>(v, tid, line, tw, lsync);
             if (a.spec2) {
                 const V* __restrict__ sp2 = a.spec2;
@@ -637,7 +651,7 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
                 else
                     apply_factors<R, E, T>(v, tid, base, lbase, nullptr, nullptr, nullptr, a.ax_real, a.axis, a.dim,
                                            a.shift, a.nmask, nullptr, key0 ^ 0x68e31da4u);
-                if (a.red.n && !a.red_at_mid)
+                if (HAS_RED && a.red.n && !a.red_at_mid)
                     accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);
             } else {  // PM_APPLY
 #pragma unroll
@@ -701,7 +715,8 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
             for (int u = 0; u < E; ++u) out[base + tid + u * T] = v[u];
         }
     }
-    if (MODE == PM_SPECRED || (a.red.n && !a.red_at_mid)) finish_red<NT>(a.red, acc);
+    if constexpr (HAS_RED)
+        if (MODE == PM_SPECRED || (a.red.n && !a.red_at_mid)) finish_red<NT>(a.red, acc);
 }
 
 // Element-wise reductions over a whole state in r-space (no transform): norm, dipole,

@@ -21,6 +21,8 @@ template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int m
     case PM_APPLY: fn = QND_PICK(PM_APPLY); break;
     case PM_DOUBLE: fn = QND_PICK(PM_DOUBLE); break;
     case PM_ROUNDTRIP: fn = QND_PICK(PM_ROUNDTRIP); break;
+    case PM_SANDWICH_RED: fn = QND_PICK(PM_SANDWICH_RED); break;
+    case PM_DOUBLE_RED: fn = QND_PICK(PM_DOUBLE_RED); break;
     default: fn = nullptr;
     }
 #undef QND_PICK
