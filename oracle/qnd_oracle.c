@@ -18,7 +18,7 @@
 #include <stdlib.h>
 #include <string.h>
 
-#define OR_MAX_DIM 3
+#define OR_MAX_DIM 6
 #define OR_MAX_EXP_ARG 700.   /* integrators.h:12 */
 #define OR_MAX_STAGES 10      /* integrators.h:13 */
 

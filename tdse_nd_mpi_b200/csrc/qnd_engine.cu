@@ -136,17 +136,17 @@ struct qnd_ctx {
     bool own_stream = false;
     bool fp64 = true;
     int dim = 0;
-    int64_t nr[MAX_DIM] = {1, 1, 1};
-    double dr[MAX_DIM] = {0, 0, 0};
+    int64_t nr[MAX_DIM] = {1, 1, 1, 1, 1, 1};
+    double dr[MAX_DIM] = {};
     int64_t n = 0;
-    int lognr[MAX_DIM] = {0, 0, 0};
-    int shift[MAX_DIM] = {0, 0, 0};
+    int lognr[MAX_DIM] = {};
+    int shift[MAX_DIM] = {};
     std::string integrator;
     double dt = 0;
     int s = 0;
     double as[20] = {0};
     double dNr = 1, dNp = 1;
-    int axoff[MAX_DIM] = {0, 0, 0};
+    int axoff[MAX_DIM] = {};
     int axtot = 0;
 
     std::vector<double> r[MAX_DIM], p[MAX_DIM];
@@ -189,6 +189,9 @@ struct qnd_ctx {
 
     int num_sms = 148;
     bool pdl = true;  // programmatic dependent launch between passes
+    // L2 residency of the full-grid factor tables: the largest access-policy window the device takes
+    // (0: off) and the bytes of L2 it sets aside for persisting lines
+    size_t l2_window_max = 0, l2_persist_bytes = 0;
     bool profiling = false;
     int64_t kernels_launched = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pairs;
@@ -499,13 +502,13 @@ struct PassSpec {
     const void* spec2 = nullptr;
     const void* mid_real = nullptr;
     const void* mid_cplx = nullptr;
-    const void* mid_ax_cplx[MAX_DIM] = {nullptr, nullptr, nullptr};
-    const void* mid_ax_real[MAX_DIM] = {nullptr, nullptr, nullptr};
+    const void* mid_ax_cplx[MAX_DIM] = {};
+    const void* mid_ax_real[MAX_DIM] = {};
     int red_at_mid = 0;
     const void* epi_real = nullptr;
     const void* epi_cplx = nullptr;
-    const void* ax_cplx[MAX_DIM] = {nullptr, nullptr, nullptr};
-    const void* ax_real[MAX_DIM] = {nullptr, nullptr, nullptr};
+    const void* ax_cplx[MAX_DIM] = {};
+    const void* ax_real[MAX_DIM] = {};
     int ax_in_prologue = 0;
     double scale = 1.0;
     int apply_acc = 0;
@@ -773,11 +776,31 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     lc.blockDim = dim3(unsigned(info.nt));
     lc.dynamicSmemBytes = info.smem;
     lc.stream = c->stream;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = c->pdl ? 1 : 0;
     lc.attrs = attr;
     lc.numAttrs = 1;
+    // the pass's full-grid factor table stays in L2 for its next use (l2_persist_setup)
+    if (c->l2_window_max) {
+        const void* tab = nullptr;
+        size_t tb = 0;
+        for (const void* t : {ps.mid_cplx, ps.pro_cplx, ps.epi_cplx})
+            if (!tab && t) tab = t, tb = size_t(c->n) * c->elem();
+        for (const void* t : {ps.mid_real, ps.pro_real, ps.epi_real})
+            if (!tab && t) tab = t, tb = size_t(c->n) * c->rsize();
+        if (tab && tb <= c->l2_window_max) {
+            // about three tables take turns in a chain (BM4): share the set-aside between them
+            const double share = double(c->l2_persist_bytes) / (3.0 * double(tb));
+            attr[1].id = cudaLaunchAttributeAccessPolicyWindow;
+            attr[1].val.accessPolicyWindow.base_ptr = const_cast<void*>(tab);
+            attr[1].val.accessPolicyWindow.num_bytes = tb;
+            attr[1].val.accessPolicyWindow.hitRatio = float(share < 1.0 ? share : 1.0);
+            attr[1].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+            attr[1].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+            lc.numAttrs = 2;
+        }
+    }
     if (c->fp64) {
         PassArgs<double> a;
         fill_args<double>(c, ps, a);
@@ -1324,7 +1347,7 @@ static void run_chain(qnd_ctx* c, void* psi, const std::vector<ChainK>& K, const
         // length-n1 inverse and element-wise work in natural order (FP64, reductions, chain end)
         auto point = [&](const Factor& f, int64_t lst, bool mask, const double* scale_dev) {
             const void *tr = nullptr, *tc = nullptr;
-            const void* axc[MAX_DIM] = {nullptr, nullptr, nullptr};
+            const void* axc[MAX_DIM] = {};
             set_factor(c, f, 0, lst, &tr, &tc, axc);
             long_point(c, psi, tr, tc, axc[0], mask ? c->mask_dev[0].p : nullptr, scale_dev);
         };
@@ -1787,12 +1810,14 @@ static void run_realtime(qnd_ctx* c, void* psi, const double* field_host, const 
 // psi <- M psi for the step masks set on the axes.
 static void apply_step_masks(qnd_ctx* c, void* psi) {
     if (c->fp64) {
-        const double* m[MAX_DIM] = {c->mask_dev[0].as<double>(), c->mask_dev[1].as<double>(), c->mask_dev[2].as<double>()};
+        const double* m[MAX_DIM];
+        for (int j = 0; j < MAX_DIM; ++j) m[j] = c->mask_dev[j].as<double>();
         long long nm[MAX_DIM];
         for (int j = 0; j < MAX_DIM; ++j) nm[j] = c->nr[j] - 1;
         launch_apply_masks<double>(c->n, static_cast<double2*>(psi), c->dim, c->shift, nm, m, c->stream);
     } else {
-        const float* m[MAX_DIM] = {c->mask_dev[0].as<float>(), c->mask_dev[1].as<float>(), c->mask_dev[2].as<float>()};
+        const float* m[MAX_DIM];
+        for (int j = 0; j < MAX_DIM; ++j) m[j] = c->mask_dev[j].as<float>();
         long long nm[MAX_DIM];
         for (int j = 0; j < MAX_DIM; ++j) nm[j] = c->nr[j] - 1;
         launch_apply_masks<float>(c->n, static_cast<float2*>(psi), c->dim, c->shift, nm, m, c->stream);
@@ -2113,9 +2138,39 @@ static void build_long_axis(qnd_ctx* c) {
     upload_f64(c, c->p_slot_dev, c->p_slot);
 }
 
+// The full-grid factor tables (potential phases, CAP decay) are read once per pass and the chain
+// cycles through a few of them (3 for BM4), so between their uses the state's traffic would push
+// them out of L2. Each pass that reads one marks it persisting through an access-policy window on
+// its launch; for that the process sets aside the device's maximum persisting L2 (a limit of this
+// process's context, released with it). QND_L2_PERSIST=0 turns this off.
+static std::mutex g_l2_mu;
+static std::set<int> g_l2_devices;
+static void l2_persist_setup(qnd_ctx* c) {
+    if (const char* e = std::getenv("QND_L2_PERSIST"))
+        if (!std::atoi(e)) return;
+    int maxp = 0, maxw = 0;
+    if (cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, c->device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, c->device) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    if (maxp <= 0 || maxw <= 0) return;
+    {
+        std::lock_guard<std::mutex> lk(g_l2_mu);
+        if (!g_l2_devices.count(c->device)) {
+            size_t cur = 0;
+            QND_CK(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
+            if (cur < size_t(maxp)) QND_CK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, size_t(maxp)));
+            g_l2_devices.insert(c->device);
+        }
+    }
+    c->l2_window_max = size_t(maxw);
+    c->l2_persist_bytes = size_t(maxp);
+}
+
 static void build_context(qnd_ctx* c, int dim, const int64_t* nr, const double* dr, const char* integrator,
                           double dt, int precision) {
-    if (dim < 1 || dim > MAX_DIM) QND_FAIL(QND_EINVAL, "dimension %d not in 1..3", dim);
+    if (dim < 1 || dim > MAX_DIM) QND_FAIL(QND_EINVAL, "dimension %d not in 1..%d", dim, MAX_DIM);
     if (precision != QND_FP64 && precision != QND_MIXED) QND_FAIL(QND_EINVAL, "unknown precision %d", precision);
     c->fp64 = precision == QND_FP64;
     c->dim = dim;
@@ -2184,6 +2239,7 @@ static void build_context(qnd_ctx* c, int dim, const int64_t* nr, const double* 
     QND_CK(cudaGetDevice(&c->device));
     QND_CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
     if (const char* e = getenv("QND_PDL")) c->pdl = atoi(e) != 0;
+    l2_persist_setup(c);
     QND_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     c->own_stream = true;
     std::vector<double> rall, pall;
@@ -2664,7 +2720,7 @@ int qnd_run_length_dev(qnd_ctx* ctx, void* psi_r_dev, const double* E_dev, int64
     if (nv > 0) QND_NEED(obs_dev);
     const bool fused = all_rspace(items);
     const bool masked = has_mask(ctx);
-    const double zero[MAX_DIM] = {0, 0, 0};
+    const double zero[MAX_DIM] = {};
     // observables that are r-space reductions of one descriptor: chunk-wide chains
     const bool chain = nv == 0 || (fused && rspace_red(ctx, items, obs_dev, 0).size() <= 1);
     const int64_t chunk = chunk_steps(ctx);
@@ -2766,7 +2822,7 @@ int qnd_observables(qnd_ctx* ctx, const void* psi_r_dev, int nobs, const char* c
     auto items = parse_obs(ctx, nobs, names, &nv);
     if (nv == 0) return QND_OK;
     QND_NEED(out_host);
-    double zero[MAX_DIM] = {0, 0, 0};
+    double zero[MAX_DIM] = {};
     ctx->obs_dev.ensure(size_t(nv) * sizeof(double) * 2);
     eval_obs(ctx, psi_r_dev, items, alpha ? alpha : zero, ctx->obs_dev.as<double>());
     QND_CK(cudaMemcpyAsync(out_host, ctx->obs_dev.p, nv * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -2801,7 +2857,7 @@ int qnd_final_spectra(qnd_ctx* ctx, const void* psi_r_dev, double r_mask_min, do
     const int d = ctx->dim;
     // kept momenta per axis (|p| <= pr_max, io_functions.c:191, :218-225) and their ranks
     std::vector<int> rank(size_t(ctx->axtot), -1);
-    int64_t npr[MAX_DIM] = {0, 0, 0};
+    int64_t npr[MAX_DIM] = {};
     for (int j = 0; j < d; ++j)
         for (int k = 0; k < int(ctx->nr[j]); ++k)
             if (std::fabs(ctx->p[j][k]) <= pr_max[j]) rank[ctx->axoff[j] + k] = int(npr[j]++);

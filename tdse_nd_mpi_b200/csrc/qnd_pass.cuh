@@ -38,7 +38,7 @@
 namespace qnd {
 
 constexpr int MAX_RED = 8;
-constexpr int MAX_DIM = 3;
+constexpr int MAX_DIM = 6;  // grid dimensions (the reference reads DIMENSION from its parameters)
 
 enum : int {
     PM_SANDWICH = 0,

@@ -11,6 +11,7 @@
 #include <stdio.h>
 
 #define QND_MAX_TOKENS 4096
+#define QND_DRV_MAX_DIM 6  /* grid dimensions the drivers take (the engine's limit) */
 
 typedef struct {
     int ntok;

@@ -31,8 +31,8 @@ static const char *const KEYS_IMAG[] = {"OUTPUT_IMAG", "DIMENSION", "DR", "NR", 
 
 typedef struct {
     int dim;
-    int64_t nr[3];
-    double dr[3];
+    int64_t nr[QND_DRV_MAX_DIM];
+    double dr[QND_DRV_MAX_DIM];
     int nstates;
     char potential[64], integrator[64], output[256];
     double dt, T;
@@ -50,8 +50,8 @@ static void read_params(const char *file, int argc, char **argv, ImagParams *P) 
     P->dt = .1;
     P->T = 100.;
     P->dim = qnd_find_dimension(&t);
-    if (P->dim < 1 || P->dim > 3) {
-        fprintf(stderr, "ERROR: DIMENSION %d is not supported (1 to 3)\n", P->dim);
+    if (P->dim < 1 || P->dim > QND_DRV_MAX_DIM) {
+        fprintf(stderr, "ERROR: DIMENSION %d is not supported (1 to %d)\n", P->dim, QND_DRV_MAX_DIM);
         exit(1);
     }
     for (int j = 0; j < P->dim; ++j) {
@@ -189,7 +189,7 @@ int main(int argc, char **argv) {
         clock_gettime(CLOCK_MONOTONIC, &t0);
         /* initial state (QuantumND_imag.c:171-177): (|r| + (i % 3)) exp(-|r|) */
         for (int64_t i = 0; i < n; ++i) {
-            int64_t ik[3] = {0, 0, 0}, idx = i;
+            int64_t ik[QND_DRV_MAX_DIM] = {0}, idx = i;
             for (int k = P.dim - 1; k >= 0; --k) {
                 ik[k] = idx % P.nr[k];
                 idx /= P.nr[k];

@@ -38,14 +38,14 @@ static const char *const KEYS_REAL[] = {"OUTPUT_IMAG", "NR", "N_STATES", "J_STAT
 
 typedef struct {
     int dim;
-    int64_t nr[3], nr_imag[3];
-    double dr[3];
+    int64_t nr[QND_DRV_MAX_DIM], nr_imag[QND_DRV_MAX_DIM];
+    double dr[QND_DRV_MAX_DIM];
     char potential[64], integrator[64], output_imag[256], gauge[32];
     int nstates, nstates_imag, nobs, nmodes, ne;
     int *j_states;
     double complex *coeffs;
     char (*obs)[64];
-    double cap[2], dt, T, dt_save, pr_max[3], r_mask[2], de;
+    double cap[2], dt, T, dt_save, pr_max[QND_DRV_MAX_DIM], r_mask[2], de;
     char (*envelope)[32];
     double *intensity, *lambda, *ellipticity, *cep, *delay, *duration, *amplitude, *frequency;
 } RealParams;
@@ -156,7 +156,7 @@ static void read_params(const char *file, int argc, char **argv, RealParams *P) 
         fclose(f);
     }
     P->dim = qnd_find_dimension(&ti);
-    if (P->dim < 1 || P->dim > 3) fail("ERROR: DIMENSION out of range (1 to 3)");
+    if (P->dim < 1 || P->dim > QND_DRV_MAX_DIM) fail("ERROR: DIMENSION out of range (1 to 6)");
     for (int j = 0; j < P->dim; ++j) {
         P->nr[j] = 256;
         P->dr[j] = .1;
@@ -531,7 +531,7 @@ int main(int argc, char **argv) {
         }
     }
     if (want_ped || want_pmd) {
-        int64_t npr[3] = {1, 1, 1};
+        int64_t npr[QND_DRV_MAX_DIM] = {1, 1, 1, 1, 1, 1};
         CK(qnd_final_spectra(q, psi_dev, P.r_mask[0], P.r_mask[1], P.pr_max, P.de, P.ne, NULL, npr, NULL));
         int64_t cnt = 1;
         for (int k = 0; k < P.dim; ++k) cnt *= npr[k];

@@ -225,3 +225,26 @@ def test_reference_loop_with_extension_observables_matches_oracle():
     # the reference's own columns are the reference's values
     c = psi.copy()
     np.testing.assert_array_equal(got[:, 1:3], r.run_length(c, E, ["dipole_r"]))
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference not compiled here (needs its sources)")
+def test_oracle_4d_bit_identical_to_reference():
+    """DIMENSION above 3: the reference allocates per dimension (parameters.c:46-48) and plans an
+    N-D transform of any rank (meshgrid.c:166-167); the restatement follows it in 4-D."""
+    dim, nr, dr = 4, (4, 4, 8, 8), (0.6, 0.5, 0.45, 0.4)
+    o = O.OracleCtx(dim, nr, dr, "BM4", 0.05, nthreads=2)
+    o.set_potential("H_3D")
+    o.set_cap(0.3, 0.7)
+    r = O.RefCtx(dim, nr, dr, "BM4", 0.05, "H_3D", (0.3, 0.7), nthreads=2)
+    psi = O.seeded_state(nr, 5)
+    E = np.random.default_rng(4).standard_normal((2, o.s, dim)) * 0.05
+    names = ["dipole_r", "dipole_v", "energy", "Lz"]
+    a, b = psi.copy(), psi.copy()
+    assert np.array_equal(o.run_length(a, E, names), r.run_length(b, E, names))
+    assert np.array_equal(a, b)
+    a, b = psi.copy(), psi.copy()
+    o.step_imag(a, 2), r.step_imag(b, 2)
+    assert np.array_equal(a, b)
+    a, b = psi.copy(), psi.copy()
+    o.step_velocity(a, E, 2), r.step_velocity(b, E, 2)
+    assert np.array_equal(a, b)
