@@ -154,4 +154,30 @@ template <typename R> void launch_apply_masks(long long n, cplx_t<R>* psi, int d
 template <typename R> void launch_add_potential(long long n, cplx_t<R>* dst, const cplx_t<R>* src, const double* vtab,
                                                 cudaStream_t st);
 
+// ---- the persistent sweep kernel (qnd_sweep.cu): recorded passes of many members in one launch
+constexpr int SWEEP_NT = 128;  // threads per CTA: every line length it takes has 128-thread pass CTAs
+// One recorded pass of one member: its arguments (PassArgs<R> in device memory), its line groups,
+// and the groups of the member's earlier passes that must be done before it starts.
+struct SweepSlot {
+    const void* args;
+    unsigned ngroups;
+    unsigned need;
+    int member;
+    int L, strided, kmode;
+};
+struct SweepArgs {
+    const SweepSlot* slots;      // in round order: pass r of every member, member by member
+    const long long* first;      // [nslots] the first item (line group) of each slot
+    int nslots;
+    long long nitems;
+    unsigned long long* next;    // item counter, zero at launch
+    unsigned* done;              // [members] groups done, zero at launch
+    int* abort_flag;             // raised when a wait runs out; zero at launch
+    int wait_tries;
+};
+// Line lengths the sweep kernel is built for (every axis of every member).
+constexpr bool sweep_length_ok(long long L) { return L == 128 || L == 256 || L == 512 || L == 1024; }
+// Cooperative launch over every resident CTA slot (at most one per item); the grid size goes to grid_out.
+template <typename R> cudaError_t launch_sweep(const SweepArgs& sa, cudaStream_t st, int num_sms, int* grid_out);
+
 }  // namespace qnd

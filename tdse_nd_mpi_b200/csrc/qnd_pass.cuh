@@ -331,8 +331,10 @@ template <int L, int T, typename X> __device__ __forceinline__ void prefetch_row
 }
 
 // Block reduction of acc[0..n) into partials, then the last CTA sums the partials in order.
+// blk / nblk: this CTA's group and the number of groups (the grid, or a persistent kernel's groups
+// of one pass).
 template <int NT>
-__device__ __forceinline__ void finish_red(const RedDesc& rd, double* acc) {
+__device__ __forceinline__ void finish_red(const RedDesc& rd, double* acc, unsigned blk, unsigned nblk) {
     constexpr int NW = NT / 32 > 0 ? NT / 32 : 1;
     __shared__ double red_s[NW][MAX_RED];
     __shared__ int is_last;
@@ -347,17 +349,17 @@ __device__ __forceinline__ void finish_red(const RedDesc& rd, double* acc) {
     if (t < rd.n) {
         double s = 0.0;
         for (int w = 0; w < NW; ++w) s += red_s[w][t];
-        rd.partials[(long long)blockIdx.x * MAX_RED + t] = s;
+        rd.partials[(long long)blk * MAX_RED + t] = s;
     }
     __threadfence();
     __syncthreads();
-    if (t == 0) is_last = (atomicAdd(rd.counter, 1u) == gridDim.x - 1);
+    if (t == 0) is_last = (atomicAdd(rd.counter, 1u) == nblk - 1);
     __syncthreads();
     if (!is_last) return;
     __threadfence();
     for (int k = 0; k < rd.n; ++k) {
         double s = 0.0;
-        for (unsigned b = t; b < gridDim.x; b += NT) s += __ldcg(rd.partials + (long long)b * MAX_RED + k);
+        for (unsigned b = t; b < nblk; b += NT) s += __ldcg(rd.partials + (long long)b * MAX_RED + k);
         s = warp_sum(s);
         if (lane == 0) red_s[wid][k] = s;
         __syncthreads();
@@ -370,6 +372,9 @@ __device__ __forceinline__ void finish_red(const RedDesc& rd, double* acc) {
         __syncthreads();
     }
     if (t == 0) *rd.counter = 0u;
+}
+template <int NT> __device__ __forceinline__ void finish_red(const RedDesc& rd, double* acc) {
+    finish_red<NT>(rd, acc, blockIdx.x, gridDim.x);
 }
 
 // Point-wise r-space factors on the E values a thread holds of one line: a full-grid table
@@ -456,16 +461,19 @@ __device__ __forceinline__ void apply_factors(cplx_t<R>* v, int tid, long long b
     }
 }
 
-template <typename R, int L, bool STRIDED, int KMODE>
-__global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
-    qnd_pass_kernel(const __grid_constant__ PassArgs<R> a) {
+// One CTA's share of a pass: line group g of ngroups (the CTA's G lines), with the dynamic shared
+// memory smem_raw. `wait` runs after the prologue (twiddles to shared memory, read-only tables to
+// L2), before the state is touched: the wait for the previous pass (programmatic dependent launch
+// in qnd_pass_kernel, the pass's dependency counter in the persistent sweep kernel).
+template <typename R, int L, bool STRIDED, int KMODE, typename Wait>
+__device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, unsigned ngroups,
+                                           unsigned char* smem_raw, Wait wait) {
     constexpr int MODE = pass_base_mode(KMODE);
     constexpr bool HAS_RED = pass_mode_reduces(KMODE);
     using V = cplx_t<R>;
     using SH = PassShape<R, L>;
     constexpr int E = SH::E, T = SH::T, G = SH::G, NT = SH::NT, LS = SH::LS;
     constexpr bool TWS = SH::TW_SMEM;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
     V* tw_s = reinterpret_cast<V*>(smem_raw);   // [TWN] stage twiddles (when they fit)
     V* lines = tw_s + SH::TWN;                   // [G][LS]
 
@@ -479,7 +487,6 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
     const int log2S = a.log2S;
     const long long smask = (1ll << log2S) - 1;
     auto line_base = [&](long long lam) { return (((lam >> log2S) * L) << log2S) + (lam & smask); };
-    const long long g = blockIdx.x;
     const long long lam = g * G + w;
     const bool active = lam < nlines;
     const long long base = line_base(active ? lam : 0);
@@ -508,8 +515,7 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
         }
     }
 
-    pdl_wait();
-    pdl_launch_dependents();
+    wait();
 
     V v[E];
     if constexpr (STRIDED) {
@@ -547,7 +553,7 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
                     double none[MAX_RED];
 #pragma unroll
                     for (int k = 0; k < MAX_RED; ++k) none[k] = 0.0;
-                    finish_red<NT>(a.red, none);
+                    finish_red<NT>(a.red, none, unsigned(g), ngroups);
                 }
                 return;
             }
@@ -631,7 +637,7 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
             }
             // finish those reductions here, so that no accumulator stays live through the second sandwich
             if constexpr (HAS_RED)
-                if (a.red_at_mid && a.red.n) finish_red<NT>(a.red, acc);
+                if (a.red_at_mid && a.red.n) finish_red<NT>(a.red, acc, unsigned(g), ngroups);
             fft_line_stages<L, E, -1, 0, TWS>(v, tid, line, tw, lsync);
             if (a.spec2) {
                 const V* __restrict__ sp2 = a.spec2;
@@ -716,7 +722,17 @@ __global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
         }
     }
     if constexpr (HAS_RED)
-        if (MODE == PM_SPECRED || (a.red.n && !a.red_at_mid)) finish_red<NT>(a.red, acc);
+        if (MODE == PM_SPECRED || (a.red.n && !a.red_at_mid)) finish_red<NT>(a.red, acc, unsigned(g), ngroups);
+}
+
+template <typename R, int L, bool STRIDED, int KMODE>
+__global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
+    qnd_pass_kernel(const __grid_constant__ PassArgs<R> a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    pass_group<R, L, STRIDED, KMODE>(a, blockIdx.x, gridDim.x, smem_raw, [] {
+        pdl_wait();
+        pdl_launch_dependents();
+    });
 }
 
 // Element-wise reductions over a whole state in r-space (no transform): norm, dipole,
