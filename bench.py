@@ -619,7 +619,8 @@ def sweep_leg(torch, steps):
     intensity log-uniform in [5e13, 3e14] W/cm^2 of an 800 nm 4-cycle sin^2 pulse (field samples from
     qnd_field_samples), norm + dipole every step. `steps` steps from the pulse's middle, timed with
     CUDA events around whole-sweep calls, each after an untimed call of the same shape: one CUDA graph
-    per chunk for all members (qnd_run_length_batch) and one stream per member."""
+    per chunk for all members (qnd_run_length_batch), one persistent kernel for all members
+    (qnd_run_length_sweep) and one stream per member."""
     from tdse_nd_mpi_b200 import Grid
     from tdse_nd_mpi_b200.batch import Member, launch, prepare, release
 
@@ -646,7 +647,7 @@ def sweep_leg(torch, steps):
     points = sum(n * n for n in [256] * 32 + [512] * 48 + [1024] * 16)
     out = {"members": len(members), "grid_points": points, "steps": steps, "precision": "mixed",
            "what": "whole-sweep calls, CUDA events around each (the call returns when all members are done)"}
-    for label, one in (("one_graph", True), ("streams", False)):
+    for label, one in (("persistent", "persistent"), ("one_graph", True), ("streams", False)):
         launch(runs, one)  # warm-up: tables, the chunk graphs of this shape
         launch(runs, one)
         torch.cuda.synchronize()

@@ -173,6 +173,17 @@ int qnd_observables_rspace_noalloc(qnd_ctx *ctx, const void *psi_r_dev, int nobs
 int qnd_run_length_batch(int count, qnd_ctx *const *ctxs, void *const *psi_r_dev, const double *const *E_dev,
                          int64_t nsteps, int nobs, const char *const *names, double *const *obs_dev);
 
+/* ---- the same sweep in one persistent kernel (no reference counterpart). Every member's passes are
+ *      recorded with the arguments qnd_run_length_dev would launch them with (chunk by chunk, as with
+ *      QND_NO_GRAPH set), then one cooperative launch per segment of 512 steps runs all of them: the
+ *      CTAs claim line groups in round order (pass r of every member, then pass r + 1) and wait, with
+ *      a bounded wait, only for the member's own previous pass, so members advance independently and
+ *      small grids fill the GPU together. Members must share one precision; every axis length is 128
+ *      to 1024 (QND_EUNSUPPORTED otherwise, or for observables beyond one fused reduction: use
+ *      qnd_run_length_batch). A wait that runs out makes the call return QND_ECUDA. Synchronises. */
+int qnd_run_length_sweep(int count, qnd_ctx *const *ctxs, void *const *psi_r_dev, const double *const *E_dev,
+                         int64_t nsteps, int nobs, const char *const *names, double *const *obs_dev);
+
 /* ---- adjoint gradient of a length-gauge run (no reference counterpart: the differentiation
  *      extension). From psi0_dev (r-space, not modified) it runs nsteps length-gauge steps with the
  *      field samples E_host [nsteps][s][dim] (the step mask applies as in qnd_run_length), evaluates

@@ -57,6 +57,8 @@ SIGNATURES = {
     "qnd_final_spectra": ([_vp, _vp, C.c_double, C.c_double, _dp, C.c_double, C.c_int, _dp, _i64p, _dp], C.c_int),
     "qnd_run_length_batch": ([C.c_int, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), _i64, C.c_int, _names,
                               C.POINTER(_vp)], C.c_int),
+    "qnd_run_length_sweep": ([C.c_int, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), _i64, C.c_int, _names,
+                              C.POINTER(_vp)], C.c_int),
     "qnd_adjoint_length": ([_vp, _vp, _dp, _i64, _dp, _i64, _dp, _dp, _vp], C.c_int),
     "qnd_adjoint_velocity": ([_vp, _vp, _dp, _i64, _dp, _i64, _dp, _dp, _vp], C.c_int),
     "qnd_field_samples": ([_vp, C.c_int, _vp, _i64, _vp, _vp, _vp, C.c_int], C.c_int),

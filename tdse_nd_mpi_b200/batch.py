@@ -75,10 +75,12 @@ def prepare(members) -> list:
     return runs
 
 
-def launch(runs, one_graph: bool = False, nsteps: int | None = None) -> None:
+def launch(runs, one_graph=False, nsteps: int | None = None) -> None:
     """Run every prepared member (nsteps of its field, default all); returns when all are done.
-    one_graph: all members through qnd_run_length_batch (needs the same nsteps and observables);
-    otherwise each member's own device loop on its own stream."""
+    one_graph: True or "graph" runs all members through qnd_run_length_batch (one CUDA graph per
+    chunk); "persistent" through qnd_run_length_sweep (one persistent kernel per 512 steps); both need
+    the same nsteps and observables for every member. Otherwise each member's own device loop runs on
+    its own stream."""
     import ctypes as C
 
     from ._lib import check, lib
@@ -90,9 +92,9 @@ def launch(runs, one_graph: bool = False, nsteps: int | None = None) -> None:
         names = runs[0][5]
         arr = lambda xs: (C.c_void_p * k)(*xs)  # noqa: E731
         cnames = (C.c_char_p * max(1, len(names)))(*[x.encode() for x in names])
-        check(lib().qnd_run_length_batch(k, arr([r[0].h for r in runs]), arr([r[1].ptr for r in runs]),
-                                         arr([r[2].data_ptr() for r in runs]), int(n[0]), len(names), cnames,
-                                         arr([r[3].data_ptr() for r in runs])))
+        fn = lib().qnd_run_length_sweep if one_graph == "persistent" else lib().qnd_run_length_batch
+        check(fn(k, arr([r[0].h for r in runs]), arr([r[1].ptr for r in runs]), arr([r[2].data_ptr() for r in runs]),
+                 int(n[0]), len(names), cnames, arr([r[3].data_ptr() for r in runs])))
     else:
         for (g, st, E, obs, nv, names), k in zip(runs, n):
             g.run_length_dev(st, E, k, names, obs if nv else None)

@@ -46,7 +46,7 @@ def _jobs():
     for name in ("qnd_aux", "qnd_engine"):
         jobs.append((os.path.join(CSRC, name + ".cu"), os.path.join(BUILD, name + ".o"), []))
     # the persistent sweep kernel, one precision per object (the longest compilations: start them first)
-    for fp64 in ((1, 0) if os.path.exists(os.path.join(CSRC, "qnd_sweep_host.enabled")) else ()):
+    for fp64 in (1, 0):
         jobs.insert(0, (os.path.join(CSRC, "qnd_sweep.cu"), os.path.join(BUILD, f"qnd_sweep_fp{64 if fp64 else 32}.o"),
                         [f"-DQND_SWEEP_FP64={fp64}"]))
     return jobs

@@ -26,6 +26,7 @@
 #include <map>
 #include <set>
 #include <tuple>
+#include <type_traits>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -130,6 +131,14 @@ constexpr size_t MAX_GRAPHS = 8;
 static std::atomic<uint64_t> g_ctx_serial{0};
 }  // namespace qnd
 
+// One pass of a member's run, recorded for the persistent sweep kernel: the pass kernel it would
+// launch (line length, stride, mode), its line groups, and its PassArgs<R> as bytes.
+struct RecordedPass {
+    int L = 0, strided = 0, kmode = 0;
+    unsigned ngroups = 0;
+    std::vector<unsigned char> args;
+};
+
 struct qnd_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -168,6 +177,12 @@ struct qnd_ctx {
     DevBuf gs_flag;
     DevBuf field_dev, field_tab, wtab_dev[MAX_DIM], spec_tmp[MAX_DIM];
     DevBuf scratch_a, scratch_b;
+    // qnd_run_length_sweep: while recorder is set, launch_pass records each pass (kind and arguments)
+    // there instead of launching it; field_view, when set, is where the chain reads its per-step field
+    // tables (a segment's tables live side by side in sweep_field)
+    std::vector<RecordedPass>* recorder = nullptr;
+    const void* field_view = nullptr;
+    DevBuf sweep_field, sweep_buf;
     DevBuf spec_rank, spec_partials, spec_out;  // final spectra: per-axis ranks, partial sums, results
     DevBuf field_out, embed_src;                // qnd_field_samples host-output staging; qnd_state_embed source
     DevBuf err_flag;                            // set by a kernel whose bounded wait ran out
@@ -737,6 +752,48 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     const PassKernelInfo info = lookup_pass(c->fp64, L, strided, kmode);
     const long long nlines = c->n / L;
     const long long ngroups = (nlines + info.G - 1) / info.G;
+    if (c->recorder) {
+        // qnd_run_length_sweep: the arguments this launch would get (per-thread staging: the sweep
+        // kernel takes its arguments from device memory), kept for the persistent kernel
+        if (!sweep_length_ok(L) || ps.vL || (kmode != PM_SANDWICH && kmode != PM_SANDWICH_RED && kmode != PM_DOUBLE &&
+                                             kmode != PM_DOUBLE_RED))
+            QND_FAIL(QND_EUNSUPPORTED, "qnd_run_length_sweep: a pass of line length %d, mode %d is outside the "
+                                       "sweep kernel (axis lengths 128 to 1024)", L, kmode);
+        RecordedPass rp;
+        rp.L = L;
+        rp.strided = strided ? 1 : 0;
+        rp.kmode = kmode;
+        rp.ngroups = unsigned(std::max<long long>(1, ngroups));
+        RedDesc red = ps.red;
+        if (red.n) {
+            ensure_red_scratch(c, rp.ngroups);
+            red.partials = c->partials.as<double>();
+            red.counter = c->counter.as<unsigned int>();
+        }
+        auto record = [&](auto& a) {
+            using A = std::remove_reference_t<decltype(a)>;
+            a.red = red;
+            a.log2S = log2S;
+            a.nlines = nlines;
+            a.use_tma = 0;
+            rp.args.resize(sizeof(A));
+            std::memcpy(rp.args.data(), &a, sizeof(A));
+        };
+        if (c->fp64) {
+            PassArgs<double> a;
+            fill_args<double>(c, ps, a);
+            a.tw = static_cast<const double2*>(tw);
+            record(a);
+        } else {
+            PassArgs<float> a;
+            fill_args<float>(c, ps, a);
+            a.tw = static_cast<const float2*>(tw);
+            record(a);
+        }
+        c->recorder->push_back(std::move(rp));
+        c->kernels_launched++;
+        return;
+    }
     const int staging = !strided ? 0 : ps.force_staging >= 0 ? ps.force_staging : staging_choice(c, ps, L, log2S);
     // per (kernel, device), shared by the contexts of every host thread
     static std::map<std::pair<const void*, int>, LaunchCfg> configured;
@@ -1234,7 +1291,7 @@ static void check_imag_clamp(qnd_ctx* c) {
 // Per-step field tables (laser phases / velocity-gauge kinetic phases) for a chunk of steps
 // from field samples already on the device.
 static void build_field_tables(qnd_ctx* c, const double* field_dev, int64_t nsteps, bool velocity,
-                               int conj_from = 1 << 30) {
+                               int conj_from = 1 << 30, void* out = nullptr) {
     FieldTableArgs fa{};
     fa.conj_from = conj_from;
     fa.field = field_dev;
@@ -1250,9 +1307,12 @@ static void build_field_tables(qnd_ctx* c, const double* field_dev, int64_t nste
     fa.ntot = c->axtot;
     for (int ia = 0; ia < c->s; ++ia) fa.h[ia] = c->as[2 * ia] + c->as[2 * ia + 1];
     fa.velocity = velocity ? 1 : 0;
-    c->field_tab.ensure(size_t(nsteps) * c->s * c->axtot * c->elem());
-    if (c->fp64) launch_field_tables<double>(fa, c->field_tab.as<double2>(), c->stream);
-    else launch_field_tables<float>(fa, c->field_tab.as<float2>(), c->stream);
+    if (!out) {
+        c->field_tab.ensure(size_t(nsteps) * c->s * c->axtot * c->elem());
+        out = c->field_tab.p;
+    }
+    if (c->fp64) launch_field_tables<double>(fa, static_cast<double2*>(out), c->stream);
+    else launch_field_tables<float>(fa, static_cast<float2*>(out), c->stream);
     c->kernels_launched++;
     QND_CK(cudaGetLastError());
 }
@@ -1266,7 +1326,8 @@ static void upload_field_chunk(qnd_ctx* c, const double* host, int64_t nsteps, b
 
 static const void* field_slice(qnd_ctx* c, int64_t st, int ia, int ax) {
     const size_t idx = (size_t(st) * c->s + ia) * c->axtot + c->axoff[ax];
-    return static_cast<const char*>(c->field_tab.p) + idx * c->elem();
+    const void* base = c->field_view ? c->field_view : c->field_tab.p;
+    return static_cast<const char*>(base) + idx * c->elem();
 }
 
 static bool has_mask(const qnd_ctx* c) {
@@ -3073,6 +3134,186 @@ int qnd_run_length_batch(int count, qnd_ctx* const* ctxs, void* const* psi_r_dev
                                        ms[i].c->stream));
     }
     join_members();
+    QND_CK(cudaGetLastError());
+    QND_API_END
+}
+
+// qnd_run_length_sweep: every member's passes recorded (the chains qnd_run_length_dev would launch,
+// chunk by chunk, with the same arguments), then run by the persistent sweep kernel (qnd_sweep.cu) in
+// one launch per segment of SWEEP_SEGMENT steps. Segments keep the recorded arguments and the field
+// tables of all their chunks in device memory at once.
+static const int64_t SWEEP_SEGMENT = 512;
+
+int qnd_run_length_sweep(int count, qnd_ctx* const* ctxs, void* const* psi_r_dev, const double* const* E_dev,
+                         int64_t nsteps, int nobs, const char* const* names, double* const* obs_dev) {
+    using namespace qnd;
+    QND_API_BEGIN
+    if (count < 1) QND_FAIL(QND_EINVAL, "qnd_run_length_sweep: count %d < 1", count);
+    QND_NEED(ctxs);
+    QND_NEED(psi_r_dev);
+    QND_NEED(E_dev);
+    if (nobs > 0) QND_NEED(names);
+    for (int i = 0; i < count; ++i) {
+        QND_NEED(ctxs[i]);
+        QND_NEED(psi_r_dev[i]);
+        QND_NEED(E_dev[i]);
+        qnd_ctx* c = ctxs[i];
+        if (c->device != ctxs[0]->device) QND_FAIL(QND_EINVAL, "qnd_run_length_sweep: members on different devices");
+        if (c->fp64 != ctxs[0]->fp64)
+            QND_FAIL(QND_EUNSUPPORTED, "qnd_run_length_sweep: members of both precisions (one kernel per precision)");
+        if (c->long1d) QND_FAIL(QND_EUNSUPPORTED, "qnd_run_length_sweep: a 1-D axis longer than 4096 points");
+        for (int j = 0; j < c->dim; ++j)
+            if (!sweep_length_ok(c->nr[j]))
+                QND_FAIL(QND_EUNSUPPORTED, "qnd_run_length_sweep: axis length %lld (the sweep kernel takes 128 to 1024)",
+                         (long long)c->nr[j]);
+        for (int j = 0; j < i; ++j)
+            if (ctxs[j] == c) QND_FAIL(QND_EINVAL, "qnd_run_length_sweep: a context appears twice");
+    }
+    if (nsteps <= 0) return QND_OK;
+    set_device(ctxs[0]);
+    std::vector<SweepMember> ms(static_cast<size_t>(count));
+    for (int i = 0; i < count; ++i) {
+        SweepMember& m = ms[i];
+        m.c = ctxs[i];
+        m.items = parse_obs(m.c, nobs, names, &m.nv);
+        if (m.nv > 0) {
+            QND_NEED(obs_dev);
+            QND_NEED(obs_dev[i]);
+        }
+        m.masked = has_mask(m.c);
+        std::vector<double> probe(size_t(m.nv) + 1);
+        if (m.nv > 0 && !(all_rspace(m.items) && rspace_red(m.c, m.items, probe.data(), 0).size() <= 1))
+            QND_FAIL(QND_EUNSUPPORTED, "qnd_run_length_sweep: observables beyond one fused reduction descriptor");
+    }
+    qnd_ctx* home = ctxs[0];
+    const size_t argsz = (size_t(home->fp64 ? sizeof(PassArgs<double>) : sizeof(PassArgs<float>)) + 127) / 128 * 128;
+    struct Ev {
+        std::vector<cudaEvent_t> e;
+        ~Ev() {
+            for (cudaEvent_t x : e)
+                if (x) cudaEventDestroy(x);
+        }
+    } ev;
+    ev.e.assign(size_t(count) + 1, nullptr);
+    for (auto& x : ev.e) QND_CK(cudaEventCreateWithFlags(&x, cudaEventDisableTiming));
+    int failed = 0;
+    for (int64_t s0 = 0; s0 < nsteps && !failed; s0 += SWEEP_SEGMENT) {
+        const int64_t seg = std::min(SWEEP_SEGMENT, nsteps - s0);
+        // record every member's chains for this segment (their field tables built on their streams)
+        std::vector<std::vector<RecordedPass>> rec(static_cast<size_t>(count));
+        for (int i = 0; i < count; ++i) {
+            SweepMember& m = ms[i];
+            qnd_ctx* c = m.c;
+            const int64_t chunk = chunk_steps(c);
+            const size_t per_step = size_t(c->s) * c->axtot * c->elem();
+            c->sweep_field.ensure(size_t(seg) * per_step);
+            for (int64_t c0 = 0; c0 < seg; c0 += chunk) {
+                const int64_t ch = std::min(chunk, seg - c0);
+                void* tabs = static_cast<char*>(c->sweep_field.p) + size_t(c0) * per_step;
+                build_field_tables(c, E_dev[i] + size_t(s0 + c0) * c->s * c->dim, ch, false, 1 << 30, tabs);
+                RedFn rf;
+                if (m.nv > 0) {
+                    double* rows = obs_dev[i] + size_t(s0 + c0) * m.nv;
+                    SweepMember* mp = &m;
+                    rf = [mp, rows](int64_t k, int ax) { return rspace_red(mp->c, mp->items, rows + size_t(k) * mp->nv, ax); };
+                }
+                c->recorder = &rec[i];
+                c->field_view = tabs;
+                try {
+                    length_steps(c, psi_r_dev[i], 0, ch, rf, m.masked);
+                } catch (...) {
+                    c->recorder = nullptr;
+                    c->field_view = nullptr;
+                    throw;
+                }
+                c->recorder = nullptr;
+                c->field_view = nullptr;
+            }
+        }
+        // slots in round order, items (line groups) numbered through them
+        size_t npass = 0, maxp = 0;
+        for (auto& r : rec) {
+            npass += r.size();
+            maxp = std::max(maxp, r.size());
+        }
+        std::vector<unsigned> need(size_t(count), 0);
+        std::vector<SweepSlot> slots;
+        std::vector<long long> first;
+        std::vector<unsigned char> blob(npass * argsz);
+        slots.reserve(npass);
+        first.reserve(npass);
+        long long nitems = 0;
+        size_t nb = 0;
+        std::vector<size_t> blob_off;
+        blob_off.reserve(npass);
+        for (size_t r = 0; r < maxp; ++r)
+            for (int i = 0; i < count; ++i) {
+                if (r >= rec[i].size()) continue;
+                const RecordedPass& p = rec[i][r];
+                std::memcpy(blob.data() + nb, p.args.data(), p.args.size());
+                SweepSlot sl{};
+                sl.ngroups = p.ngroups;
+                sl.need = need[i];
+                sl.member = i;
+                sl.L = p.L;
+                sl.strided = p.strided;
+                sl.kmode = p.kmode;
+                slots.push_back(sl);
+                blob_off.push_back(nb);
+                first.push_back(nitems);
+                nitems += p.ngroups;
+                need[i] += p.ngroups;
+                nb += argsz;
+            }
+        // device layout: [args blob][slots][first][done (count) | next | abort]
+        const size_t o_slots = (nb + 255) / 256 * 256;
+        const size_t o_first = (o_slots + slots.size() * sizeof(SweepSlot) + 255) / 256 * 256;
+        const size_t o_ctl = (o_first + first.size() * sizeof(long long) + 255) / 256 * 256;
+        const size_t ctl_bytes = (size_t(count) * sizeof(unsigned) + 15) / 16 * 16 + 16 + 16;
+        home->sweep_buf.ensure(o_ctl + ctl_bytes);
+        char* dbuf = static_cast<char*>(home->sweep_buf.p);
+        for (size_t q = 0; q < slots.size(); ++q) slots[q].args = dbuf + blob_off[q];
+        // every member's earlier work (state, tables) before the sweep's stream reads it
+        for (int i = 0; i < count; ++i) {
+            QND_CK(cudaEventRecord(ev.e[i], ms[i].c->stream));
+            QND_CK(cudaStreamWaitEvent(home->stream, ev.e[i], 0));
+        }
+        QND_CK(cudaMemcpyAsync(dbuf, blob.data(), nb, cudaMemcpyHostToDevice, home->stream));
+        QND_CK(cudaMemcpyAsync(dbuf + o_slots, slots.data(), slots.size() * sizeof(SweepSlot), cudaMemcpyHostToDevice,
+                               home->stream));
+        QND_CK(cudaMemcpyAsync(dbuf + o_first, first.data(), first.size() * sizeof(long long), cudaMemcpyHostToDevice,
+                               home->stream));
+        QND_CK(cudaMemsetAsync(dbuf + o_ctl, 0, ctl_bytes, home->stream));
+        SweepArgs sa{};
+        sa.slots = reinterpret_cast<const SweepSlot*>(dbuf + o_slots);
+        sa.first = reinterpret_cast<const long long*>(dbuf + o_first);
+        sa.nslots = int(slots.size());
+        sa.nitems = nitems;
+        sa.done = reinterpret_cast<unsigned*>(dbuf + o_ctl);
+        const size_t o_next = (size_t(count) * sizeof(unsigned) + 15) / 16 * 16;
+        sa.next = reinterpret_cast<unsigned long long*>(dbuf + o_ctl + o_next);
+        sa.abort_flag = reinterpret_cast<int*>(dbuf + o_ctl + o_next + 16);
+        sa.wait_tries = 1 << 22;  // ~1 s of polling per item before the launch gives up
+        int grid = 0;
+        const cudaError_t le = home->fp64 ? launch_sweep<double>(sa, home->stream, home->num_sms, &grid)
+                                          : launch_sweep<float>(sa, home->stream, home->num_sms, &grid);
+        if (le != cudaSuccess) {
+            cudaGetLastError();
+            QND_FAIL(QND_ECUDA, "qnd_run_length_sweep: launch of the sweep kernel: %s", cudaGetErrorString(le));
+        }
+        // the members' later work after the sweep; the blob and tables are reused by the next segment
+        QND_CK(cudaEventRecord(ev.e[count], home->stream));
+        for (int i = 0; i < count; ++i) QND_CK(cudaStreamWaitEvent(ms[i].c->stream, ev.e[count], 0));
+        QND_CK(cudaMemcpyAsync(&failed, sa.abort_flag, sizeof(int), cudaMemcpyDeviceToHost, home->stream));
+        QND_CK(cudaStreamSynchronize(home->stream));
+    }
+    if (failed) {
+        // a wait ran out: the skipped groups' reductions never finished; clear their ticket counters
+        for (SweepMember& m : ms)
+            if (m.c->counter.p) QND_CK(cudaMemsetAsync(m.c->counter.p, 0, m.c->counter.bytes, m.c->stream));
+        for (SweepMember& m : ms) QND_CK(cudaStreamSynchronize(m.c->stream));
+        QND_FAIL(QND_ECUDA, "qnd_run_length_sweep: a wait for a member's previous pass ran out; results are invalid");
+    }
     QND_CK(cudaGetLastError());
     QND_API_END
 }

@@ -144,3 +144,46 @@ def test_contexts_on_several_host_threads_match_one_thread(qnd_lib):
     for a, b in zip(alone, got):
         np.testing.assert_array_equal(a["obs"], b["obs"])
         np.testing.assert_array_equal(a["psi"], b["psi"])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_persistent_sweep_matches_members_alone(qnd_lib, precision, monkeypatch):
+    """qnd_run_length_sweep (one persistent kernel over every member's passes) over uneven grids,
+    square and not, BM4 and Verlet members, 300 steps (chunks of 128, 128 and 44 steps): every
+    member's rows and final state equal its own run_length_dev with direct launches, bit for bit."""
+    import dataclasses
+
+    from tdse_nd_mpi_b200.batch import run_members
+
+    def sweep_member(shape, seed, integ="BM4"):
+        m = _member(shape, seed, integ)
+        rng = np.random.default_rng(200 + seed)
+        s = 1 if integ == "Verlet" else 6
+        return dataclasses.replace(m, field=rng.standard_normal((300, s, len(shape))) * 0.05, precision=precision)
+
+    members = [sweep_member((128, 128), 31), sweep_member((256, 128), 32, "Verlet"), sweep_member((256, 256), 33),
+               sweep_member((128, 512), 34, "Verlet"), sweep_member((512, 512), 35)]
+    together = run_members(members, one_graph="persistent")
+    monkeypatch.setenv("QND_NO_GRAPH", "1")
+    alone = run_members(members, one_graph=False)
+    for a, b in zip(together, alone):
+        np.testing.assert_array_equal(a["obs"], b["obs"])
+        np.testing.assert_array_equal(a["psi"], b["psi"])
+
+
+@pytest.mark.gpu
+def test_persistent_sweep_refuses_what_it_does_not_hold(qnd_lib):
+    """Axis lengths outside 128..1024 and mixed precisions give QND_EUNSUPPORTED (no launch)."""
+    from tdse_nd_mpi_b200 import QndError
+    from tdse_nd_mpi_b200.batch import launch, prepare, release
+
+    for members in ([_member((64, 128), 41)], [_member((128, 128), 42), _member((128, 128), 43)]):
+        if len(members) == 2:
+            import dataclasses
+            members[1] = dataclasses.replace(members[1], precision="mixed")
+        runs = prepare(members)
+        with pytest.raises(QndError) as ei:
+            launch(runs, "persistent")
+        assert ei.value.code == 5
+        release(runs)
