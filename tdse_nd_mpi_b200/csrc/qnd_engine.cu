@@ -204,9 +204,6 @@ struct qnd_ctx {
 
     int num_sms = 148;
     bool pdl = true;  // programmatic dependent launch between passes
-    // L2 residency of the full-grid factor tables: the largest access-policy window the device takes
-    // (0: off) and the bytes of L2 it sets aside for persisting lines
-    size_t l2_window_max = 0, l2_persist_bytes = 0;
     bool profiling = false;
     int64_t kernels_launched = 0;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> prof_pairs;
@@ -276,16 +273,19 @@ static void round_pairs_f32_balanced(const double* v, size_t n, float* out) {
     }
 }
 
-// Twiddles of HostPlan(L) in the [j mod Ns][r-1] layout, exp(-2 pi i jm r / (Ns R)), in long double.
+// Stage twiddles of HostPlan(L), exp(-2 pi i jm r / (Ns R)) in long double: FP64 plans one base per
+// butterfly position (r = 1; the kernel forms the powers, pow_twiddles), FP32 plans every r in the
+// [j mod Ns][r-1] layout.
 static void build_twiddles(qnd_ctx* c, int L, DevBuf& dst) {
     HostPlan pl(L, lookup_pass(c->fp64, L, false, PM_SANDWICH).E);
-    std::vector<double> tw(2 * size_t(pl.tw_size > 0 ? pl.tw_size : 1));
+    const int entries = c->fp64 ? pl.twb_size : pl.tw_size;
+    std::vector<double> tw(2 * size_t(entries > 0 ? entries : 1));
     const long double two_pi = 6.283185307179586476925286766559005768L;
     size_t o = 0;
     for (int st = 1; st < pl.nstage; ++st) {
         const int R = pl.radix[st], Ns = pl.span[st];
         for (int jm = 0; jm < Ns; ++jm)
-            for (int r = 1; r < R; ++r) {
+            for (int r = 1; r < (c->fp64 ? 2 : R); ++r) {
                 long double ang = two_pi * (long double)(jm * r) / (long double)(Ns * R);
                 if (c->fp64) {
                     tw[2 * o] = (double)cosl(ang);
@@ -297,7 +297,7 @@ static void build_twiddles(qnd_ctx* c, int L, DevBuf& dst) {
                 ++o;
             }
     }
-    const size_t cnt = size_t(pl.tw_size > 0 ? pl.tw_size : 1);
+    const size_t cnt = size_t(entries > 0 ? entries : 1);
     dst.ensure(cnt * c->elem());
     if (c->fp64) {
         QND_CK(cudaMemcpyAsync(dst.p, tw.data(), cnt * 16, cudaMemcpyHostToDevice, c->stream));
@@ -747,6 +747,8 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     // passes that reduce run the instantiation that carries the reduction code; the others keep its
     // registers for the transform
     int kmode = ps.mode;
+    if (ps.red.n && ps.mode == PM_DOUBLE && !ps.red_at_mid)
+        QND_FAIL(QND_EINVAL, "internal: a two-sandwich pass reduces between its sandwiches only");
     if (ps.red.n && ps.mode == PM_SANDWICH) kmode = PM_SANDWICH_RED;
     if (ps.red.n && ps.mode == PM_DOUBLE) kmode = PM_DOUBLE_RED;
     const PassKernelInfo info = lookup_pass(c->fp64, L, strided, kmode);
@@ -833,31 +835,11 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     lc.blockDim = dim3(unsigned(info.nt));
     lc.dynamicSmemBytes = info.smem;
     lc.stream = c->stream;
-    cudaLaunchAttribute attr[2];
+    cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = c->pdl ? 1 : 0;
     lc.attrs = attr;
     lc.numAttrs = 1;
-    // the pass's full-grid factor table stays in L2 for its next use (l2_persist_setup)
-    if (c->l2_window_max) {
-        const void* tab = nullptr;
-        size_t tb = 0;
-        for (const void* t : {ps.mid_cplx, ps.pro_cplx, ps.epi_cplx})
-            if (!tab && t) tab = t, tb = size_t(c->n) * c->elem();
-        for (const void* t : {ps.mid_real, ps.pro_real, ps.epi_real})
-            if (!tab && t) tab = t, tb = size_t(c->n) * c->rsize();
-        if (tab && tb <= c->l2_window_max) {
-            // about three tables take turns in a chain (BM4): share the set-aside between them
-            const double share = double(c->l2_persist_bytes) / (3.0 * double(tb));
-            attr[1].id = cudaLaunchAttributeAccessPolicyWindow;
-            attr[1].val.accessPolicyWindow.base_ptr = const_cast<void*>(tab);
-            attr[1].val.accessPolicyWindow.num_bytes = tb;
-            attr[1].val.accessPolicyWindow.hitRatio = float(share < 1.0 ? share : 1.0);
-            attr[1].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
-            attr[1].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
-            lc.numAttrs = 2;
-        }
-    }
     if (c->fp64) {
         PassArgs<double> a;
         fill_args<double>(c, ps, a);
@@ -2199,36 +2181,6 @@ static void build_long_axis(qnd_ctx* c) {
     upload_f64(c, c->p_slot_dev, c->p_slot);
 }
 
-// The full-grid factor tables (potential phases, CAP decay) are read once per pass and the chain
-// cycles through a few of them (3 for BM4), so between their uses the state's traffic would push
-// them out of L2. Each pass that reads one marks it persisting through an access-policy window on
-// its launch; for that the process sets aside the device's maximum persisting L2 (a limit of this
-// process's context, released with it). QND_L2_PERSIST=0 turns this off.
-static std::mutex g_l2_mu;
-static std::set<int> g_l2_devices;
-static void l2_persist_setup(qnd_ctx* c) {
-    if (const char* e = std::getenv("QND_L2_PERSIST"))
-        if (!std::atoi(e)) return;
-    int maxp = 0, maxw = 0;
-    if (cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, c->device) != cudaSuccess ||
-        cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, c->device) != cudaSuccess) {
-        cudaGetLastError();
-        return;
-    }
-    if (maxp <= 0 || maxw <= 0) return;
-    {
-        std::lock_guard<std::mutex> lk(g_l2_mu);
-        if (!g_l2_devices.count(c->device)) {
-            size_t cur = 0;
-            QND_CK(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
-            if (cur < size_t(maxp)) QND_CK(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, size_t(maxp)));
-            g_l2_devices.insert(c->device);
-        }
-    }
-    c->l2_window_max = size_t(maxw);
-    c->l2_persist_bytes = size_t(maxp);
-}
-
 static void build_context(qnd_ctx* c, int dim, const int64_t* nr, const double* dr, const char* integrator,
                           double dt, int precision) {
     if (dim < 1 || dim > MAX_DIM) QND_FAIL(QND_EINVAL, "dimension %d not in 1..%d", dim, MAX_DIM);
@@ -2300,7 +2252,6 @@ static void build_context(qnd_ctx* c, int dim, const int64_t* nr, const double* 
     QND_CK(cudaGetDevice(&c->device));
     QND_CK(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device));
     if (const char* e = getenv("QND_PDL")) c->pdl = atoi(e) != 0;
-    l2_persist_setup(c);
     QND_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     c->own_stream = true;
     std::vector<double> rall, pall;

@@ -218,8 +218,39 @@ template <int L, int E> struct FFTPlan {
         return st <= 1 ? 0 : tw_offset(st - 1) + span(st - 1) * (radix(st - 1) - 1);
     }
     __host__ __device__ static constexpr int tw_size() { return tw_offset(NSTAGE) ; }
+    // FP64 plans store one base twiddle per butterfly position, W_{Ns R}^{jm} for jm < Ns, and form
+    // its powers in registers (pow_twiddles): stage st's bases start at twb_offset(st)
+    __host__ __device__ static constexpr int twb_offset(int st) {
+        return st <= 1 ? 0 : twb_offset(st - 1) + span(st - 1);
+    }
+    __host__ __device__ static constexpr int twb_size() { return twb_offset(NSTAGE); }
     static constexpr int SMEM_LINE = L + L / E;  // padded values per line (before line padding)
 };
+
+// Multiply u[1..R-1] by w^1 .. w^(R-1) with w the base twiddle of the butterfly (FP64 plans). The
+// powers are formed as w^(4k + j) = w^(4k) w^j from w, w^2, w^3 and the running w^(4k) (w^4, w^8 =
+// (w^4)^2, w^12 = w^8 w^4): at most four rounded products deep, about four units in the last place,
+// against one shared-memory load per twiddle in the table form. Trades shared-memory bandwidth, the
+// bound of the transform's exchanges, for FP64 multiplies.
+template <int R, typename V> __device__ __forceinline__ void pow_twiddles(V* u, V w) {
+    if constexpr (R >= 2) u[1] = cmul(u[1], w);
+    if constexpr (R >= 4) {
+        const V w2 = cmul(w, w);
+        const V w3 = cmul(w2, w);
+        u[2] = cmul(u[2], w2);
+        u[3] = cmul(u[3], w3);
+        const V w4 = cmul(w2, w2);
+        V w4k = w4;
+#pragma unroll
+        for (int k = 1; k < R / 4; ++k) {
+            u[4 * k] = cmul(u[4 * k], w4k);
+            u[4 * k + 1] = cmul(u[4 * k + 1], cmul(w4k, w));
+            u[4 * k + 2] = cmul(u[4 * k + 2], cmul(w4k, w2));
+            u[4 * k + 3] = cmul(u[4 * k + 3], cmul(w4k, w3));
+            if (k + 1 < R / 4) w4k = (k == 1) ? cmul(w4, w4) : cmul(w4k, w4);
+        }
+    }
+}
 
 // One Stockham stage on the thread's E registers (B = E/R butterflies, j = tid + b*T).
 // Input registers hold x[j + r*L/R] for butterfly b at v[b*R + r]; output registers hold
@@ -238,14 +269,23 @@ __device__ __forceinline__ void fft_stage_regs(V* v, int tid, const V* __restric
         if constexpr (Ns > 1) {
             const int j = tid + b * P::T;
             const int jm = j & (Ns - 1);
-            const V* t = tw + P::tw_offset(ST) + jm * (R - 1);
-#pragma unroll
-            for (int r = 1; r < R; ++r) {
+            if constexpr (sizeof(u[0].x) == 8) {
+                const V* t = tw + P::twb_offset(ST) + jm;
                 V w;
-                if constexpr (TWS) w = t[r - 1];
-                else w = __ldg(t + r - 1);
+                if constexpr (TWS) w = *t;
+                else w = __ldg(t);
                 if constexpr (SIGN > 0) w.y = -w.y;
-                u[r] = fmul(u[r], w);
+                pow_twiddles<R>(u, w);
+            } else {
+                const V* t = tw + P::tw_offset(ST) + jm * (R - 1);
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    V w;
+                    if constexpr (TWS) w = t[r - 1];
+                    else w = __ldg(t + r - 1);
+                    if constexpr (SIGN > 0) w.y = -w.y;
+                    u[r] = fmul(u[r], w);
+                }
             }
         }
         RegDFT<R, SIGN>::run(u);

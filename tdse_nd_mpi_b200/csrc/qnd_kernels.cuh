@@ -21,7 +21,8 @@ template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int m
 struct HostPlan {
     int L, E, T, nstage;
     int radix[16], span[16];
-    int tw_size;
+    int tw_size;   // table form (FP32): R - 1 twiddles per butterfly position
+    int twb_size;  // base form (FP64): one twiddle per butterfly position
     HostPlan(int L_, int E_) : L(L_) {
         E = E_;
         T = L / E;
@@ -31,10 +32,12 @@ struct HostPlan {
         nstage = loge ? (logl + loge - 1) / loge : 1;
         int ns = 1;
         tw_size = 0;
+        twb_size = 0;
         for (int st = 0; st < nstage; ++st) {
             radix[st] = st < nstage - 1 ? E : (1 << (logl - loge * (nstage - 1)));
             span[st] = ns;
             if (st >= 1) tw_size += ns * (radix[st] - 1);
+            if (st >= 1) twb_size += ns;
             ns *= radix[st];
         }
     }

@@ -142,7 +142,9 @@ template <typename R, int L> struct PassShape {
     static constexpr int LS_TARGET = G >= SLOTS ? 1 : SLOTS / G;
     static constexpr int LINE_RAW = FFTPlan<L, E>::SMEM_LINE;
     static constexpr int LS = LINE_RAW + ((LS_TARGET - LINE_RAW % SLOTS) % SLOTS + SLOTS) % SLOTS;
-    static constexpr int TWN_RAW = (FFTPlan<L, E>::tw_size() + 1) & ~1;
+    // stage twiddle entries: FP64 plans keep one base per butterfly position (pow_twiddles)
+    static constexpr int TW_ENTRIES = sizeof(R) == 8 ? FFTPlan<L, E>::twb_size() : FFTPlan<L, E>::tw_size();
+    static constexpr int TWN_RAW = (TW_ENTRIES + 1) & ~1;
     // stage twiddles in shared memory when they are small and shared by several lines of the CTA;
     // otherwise read them through L1 (one copy per SM instead of one per CTA)
     static constexpr bool TW_SMEM = G > 1 && size_t(TWN_RAW) * sizeof(cplx_t<R>) <= 16 * 1024;
@@ -496,7 +498,7 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
 
     const V* tw = a.tw;
     if constexpr (TWS) {
-        for (int i = t; i < FFTPlan<L, E>::tw_size(); i += NT) tw_s[i] = a.tw[i];
+        for (int i = t; i < SH::TW_ENTRIES; i += NT) tw_s[i] = a.tw[i];
         tw = tw_s;
     }
 
@@ -598,7 +600,7 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
 
     if constexpr (MODE == PM_FFT_INV || MODE == PM_ROUNDTRIP) {
         fft_line_stages<L, E, +1, 0, TWS>(v, tid, line, tw, lsync);
-    } else {
+    } else if constexpr (MODE != PM_DOUBLE) {
         fft_line_stages<L, E, -1, 0, TWS>(v, tid, line, tw, lsync);
     }
 
@@ -617,8 +619,49 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
         store_out = true;
     } else if constexpr (MODE == PM_SPECRED) {
         if (active) accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);
+    } else if constexpr (MODE == PM_DOUBLE) {
+        // The two sandwiches along the same axis as two turns of one loop, the r-space factor (and
+        // the reductions of a step boundary) after the first: the code of each transform direction
+        // exists once, so that the pass fits the instruction cache of the SM. The reducing variant
+        // (one pass per step) is unrolled: its accumulators would otherwise stay live in the loop.
+        constexpr int TURNS_UNROLLED = HAS_RED ? 2 : 1;
+#pragma unroll TURNS_UNROLLED
+        for (int half = 0; half < 2; ++half) {
+            fft_line_stages<L, E, -1, 0, TWS>(v, tid, line, tw, lsync);
+            const V* __restrict__ sp = half ? a.spec2 : (a.spec ? a.spec + (a.spec_full ? lbase : 0ll) : nullptr);
+            if (sp) {
+                const uint32_t kh = key0 + uint32_t(half * L);
+#pragma unroll
+                for (int u = 0; u < E; ++u)
+                    v[u] = fmul_spec<L>(v[u], __ldg(sp + tid + u * T), kh + uint32_t(tid + u * T), u == 0 || u == E - 1);
+            }
+            fft_line_stages<L, E, +1, 0, TWS>(v, tid, line, tw, lsync);
+            if (half == 0) {
+                if (active) {
+                    apply_factors<R, E, T>(v, tid, base, lbase, a.mid_real, a.mid_cplx, a.mid_ax_cplx, a.mid_ax_real,
+                                           a.axis, a.dim, a.shift, a.nmask, nullptr, key0 ^ 0x2545f491u);
+                    // a step boundary inside the pass: observables of the state between the two steps
+                    if (HAS_RED && a.red_at_mid && a.red.n)
+                        accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift,
+                                                 a.nmask);
+                }
+                // finish those reductions here, so that no accumulator stays live through the second sandwich
+                if constexpr (HAS_RED)
+                    if (a.red_at_mid && a.red.n) finish_red<NT>(a.red, acc, unsigned(g), ngroups);
+            }
+        }
+        if (active) {
+            if (a.epi_real || a.epi_cplx || !a.ax_in_prologue)
+                apply_factors<R, E, T>(v, tid, base, lbase, a.epi_real, a.epi_cplx, a.ax_in_prologue ? nullptr : a.ax_cplx,
+                                       a.ax_real, a.axis, a.dim, a.shift, a.nmask, nullptr, key0 ^ 0x68e31da4u);
+            else
+                apply_factors<R, E, T>(v, tid, base, lbase, nullptr, nullptr, nullptr, a.ax_real, a.axis, a.dim,
+                                       a.shift, a.nmask, nullptr, key0 ^ 0x68e31da4u);
+            // (a two-sandwich pass reduces only between its sandwiches: red_at_mid, checked by the host)
+        }
+        store_out = true;
     } else {
-        // SANDWICH / DOUBLE / APPLY: spectral multiply, inverse transform
+        // SANDWICH / APPLY: spectral multiply, inverse transform
         if (a.spec) {
             const V* __restrict__ sp = a.spec + (a.spec_full ? lbase : 0ll);
 #pragma unroll
@@ -626,28 +669,6 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
                 v[u] = fmul_spec<L>(v[u], __ldg(sp + tid + u * T), key0 + uint32_t(tid + u * T), u == 0 || u == E - 1);
         }
         fft_line_stages<L, E, +1, 0, TWS>(v, tid, line, tw, lsync);
-        if constexpr (MODE == PM_DOUBLE) {
-            // r-space factor between the two sandwiches, then the second sandwich on the same axis
-            if (active) {
-                apply_factors<R, E, T>(v, tid, base, lbase, a.mid_real, a.mid_cplx, a.mid_ax_cplx, a.mid_ax_real,
-                                       a.axis, a.dim, a.shift, a.nmask, nullptr, key0 ^ 0x2545f491u);
-                // a step boundary inside the pass: observables of the state between the two steps
-                if (HAS_RED && a.red_at_mid && a.red.n)
-                    accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);
-            }
-            // finish those reductions here, so that no accumulator stays live through the second sandwich
-            if constexpr (HAS_RED)
-                if (a.red_at_mid && a.red.n) finish_red<NT>(a.red, acc, unsigned(g), ngroups);
-            fft_line_stages<L, E, -1, 0, TWS>(v, tid, line, tw, lsync);
-            if (a.spec2) {
-                const V* __restrict__ sp2 = a.spec2;
-#pragma unroll
-                for (int u = 0; u < E; ++u)
-                    v[u] = fmul_spec<L>(v[u], __ldg(sp2 + tid + u * T), key0 + uint32_t(L + tid + u * T),
-                                        u == 0 || u == E - 1);
-            }
-            fft_line_stages<L, E, +1, 0, TWS>(v, tid, line, tw, lsync);
-        }
         if (active) {
             if constexpr (PROPAGATE) {
                 if (a.epi_real || a.epi_cplx || !a.ax_in_prologue)
@@ -721,7 +742,7 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
             for (int u = 0; u < E; ++u) out[base + tid + u * T] = v[u];
         }
     }
-    if constexpr (HAS_RED)
+    if constexpr (HAS_RED && MODE != PM_DOUBLE)
         if (MODE == PM_SPECRED || (a.red.n && !a.red_at_mid)) finish_red<NT>(a.red, acc, unsigned(g), ngroups);
 }
 

@@ -26,7 +26,7 @@ template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int m
     default: fn = nullptr;
     }
 #undef QND_PICK
-    return PassKernelInfo{fn, SH::NT, SH::SMEM, SH::G, FFTPlan<L, SH::E>::tw_size(), SH::E};
+    return PassKernelInfo{fn, SH::NT, SH::SMEM, SH::G, SH::TW_ENTRIES, SH::E};
 }
 
 template PassKernelInfo pass_kernel_info<double, QND_L>(bool, int);
