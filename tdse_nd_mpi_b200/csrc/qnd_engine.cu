@@ -95,10 +95,10 @@ struct DevBuf {
     template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
-static PassKernelInfo lookup_pass(bool fp64, int L, bool strided, int mode) {
+static PassKernelInfo lookup_pass(bool fp64, int L, bool strided, int mode, int var = 0) {
 #define QND_CASE(LL)                                                                                              \
     case LL:                                                                                                      \
-        return fp64 ? pass_kernel_info<double, LL>(strided, mode) : pass_kernel_info<float, LL>(strided, mode);
+        return fp64 ? pass_kernel_info<double, LL>(strided, mode, var) : pass_kernel_info<float, LL>(strided, mode, var);
     switch (L) {
         QND_CASE(2) QND_CASE(4) QND_CASE(8) QND_CASE(16) QND_CASE(32) QND_CASE(64) QND_CASE(128) QND_CASE(256)
         QND_CASE(512) QND_CASE(1024) QND_CASE(2048) QND_CASE(4096)
@@ -236,9 +236,19 @@ namespace qnd {
 // by two single-entry errors in total, so the FFT stage twiddles and the phase tables applied at
 // every step leave no systematic drift of the norm. Each part stays within two units in the last
 // place.
+// QND_F32_TABLES selects another rounding for experiments: "nearest" (each part to nearest) or
+// "magnitude" (per entry the candidate pair whose |1 + d|^2 is closest, no running sum).
 static void round_pairs_f32_balanced(const double* v, size_t n, float* out) {
+    const char* mode = std::getenv("QND_F32_TABLES");
+    const bool nearest = mode && !std::strcmp(mode, "nearest");
+    const bool per_entry = mode && !std::strcmp(mode, "magnitude");
+    if (nearest) {
+        for (size_t i = 0; i < 2 * n; ++i) out[i] = float(v[i]);
+        return;
+    }
     double run = 0.0;
     for (size_t i = 0; i < n; ++i) {
+        if (per_entry) run = 0.0;
         const double re = v[2 * i], im = v[2 * i + 1];
         // |1 + x|^2 - |1 + d|^2 = (xr - dr)(2 + xr + dr) + (xi - di)(xi + di)
         auto merr = [&](double xr, double xi) { return (xr - re) * (2.0 + xr + re) + (xi - im) * (xi + im); };
@@ -531,6 +541,7 @@ struct PassSpec {
     RedDesc red{};
     int spec_full = 0;           // spec: a full-grid table in line-major order
     int force_staging = -1;      // strided passes: -1 the tuned staging, 0 per-thread copies, 1 TMA boxes
+    int force_shape = -1;        // -1 the tuned shape variant (shape_choice), else that variant
     // a pass over a virtual axis of a long 1-D axis: its length, log2 stride and stage twiddles
     int vL = 0, vlog2S = 0;
     const void* vtw = nullptr;
@@ -628,7 +639,7 @@ static bool strided_tma_map(qnd_ctx* c, const void* psi, int L, int log2S, int G
     const int64_t S = int64_t(1) << log2S;
     const size_t ce = c->elem();
     if (reinterpret_cast<uintptr_t>(psi) % 16 || S < G || (size_t(G) * ce) % 16 || (c->n / L) % G) return false;
-    const auto key = std::make_tuple(psi, L, log2S);
+    const auto key = std::make_tuple(psi, L * 64 + G, log2S);  // G <= 32 lines per box
     auto it = c->tmaps.find(key);
     if (it != c->tmaps.end()) {
         *map = it->second;
@@ -736,6 +747,89 @@ static void check_device_error(qnd_ctx* c) {
     }
 }
 
+// Tile-shape autotuner. The sandwich and two-sandwich passes of lines of 256 to 2048 points are
+// built in NSHAPES shapes (PassShape: the default, half and twice the lines per CTA). Per (device,
+// precision, points, line length, stride, pass kind) the first launch outside a stream capture times
+// the pass itself with each shape (its reductions left out) on a zeroed scratch state: one warm-up
+// and three launches each, untimed by the launch counters. A variant replaces the default only when
+// it is at least 2% faster. Every line is transformed the same way in every shape, so a pass without
+// reductions gives the same bits in each; the shape changes only how the partial sums of a reduction
+// are grouped (the CTA count), a rounding-level difference. The choice holds for the whole process,
+// so repeated runs agree bit for bit. QND_SHAPE=<v> forces a variant where it exists; QND_TUNE=0
+// keeps the default; QND_TUNE_LOG=<file> appends every measurement to that file.
+struct ShapeKey {
+    int device, fp64;
+    long long n;
+    int L, log2S, mode;
+    bool operator<(const ShapeKey& o) const {
+        return std::tie(device, fp64, n, L, log2S, mode) < std::tie(o.device, o.fp64, o.n, o.L, o.log2S, o.mode);
+    }
+};
+static std::mutex g_shape_mu;
+static std::map<ShapeKey, int> g_shape;
+
+static int shape_choice(qnd_ctx* c, const PassSpec& ps, int L, int log2S, int kmode) {
+    const int mode = pass_base_mode(kmode);
+    if (ps.vL || (mode != PM_SANDWICH && mode != PM_DOUBLE) || L < 256 || L > 2048) return 0;
+    const bool strided = log2S > 0;
+    if (const char* f = std::getenv("QND_SHAPE")) {
+        const int v = std::atoi(f);
+        if (v > 0 && v < NSHAPES && lookup_pass(c->fp64, L, strided, kmode, v).fn) return v;
+        return 0;
+    }
+    const ShapeKey key{c->device, int(c->fp64), c->n, L, log2S, mode};
+    {
+        std::lock_guard<std::mutex> lk(g_shape_mu);
+        auto it = g_shape.find(key);
+        if (it != g_shape.end()) return it->second;
+    }
+    const char* tune = std::getenv("QND_TUNE");
+    if ((tune && !std::atoi(tune)) || c->profiling) return 0;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    QND_CK(cudaStreamIsCapturing(c->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return 0;
+    c->tune_buf.ensure(size_t(c->n) * c->elem());
+    QND_CK(cudaMemsetAsync(c->tune_buf.p, 0, size_t(c->n) * c->elem(), c->stream));
+    PassSpec t = ps;
+    t.mode = mode;
+    t.red = RedDesc{};
+    t.red_at_mid = 0;
+    t.psi = c->tune_buf.p;
+    const int64_t k0 = c->kernels_launched;
+    cudaEvent_t e0, e1;
+    QND_CK(cudaEventCreate(&e0));
+    QND_CK(cudaEventCreate(&e1));
+    float ms[NSHAPES];
+    int choice = 0;
+    for (int v = 0; v < NSHAPES; ++v) {
+        ms[v] = -1.f;
+        if (!lookup_pass(c->fp64, L, strided, mode, v).fn) continue;
+        t.force_shape = v;
+        launch_pass(c, t);
+        QND_CK(cudaEventRecord(e0, c->stream));
+        for (int r = 0; r < 3; ++r) launch_pass(c, t);
+        QND_CK(cudaEventRecord(e1, c->stream));
+        QND_CK(cudaEventSynchronize(e1));
+        QND_CK(cudaEventElapsedTime(&ms[v], e0, e1));
+        if (v > 0 && ms[v] < 0.98f * ms[choice]) choice = v;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->kernels_launched = k0;
+    c->tune_buf.reset();
+    if (const char* logf = std::getenv("QND_TUNE_LOG")) {
+        if (FILE* f = std::fopen(logf, "a")) {
+            std::fprintf(f, "%s\tn=%lld\tL=%d\tlog2S=%d\t%s\tms=%.4f,%.4f,%.4f\tchoice=%d\n", c->fp64 ? "fp64" : "fp32",
+                         (long long)c->n, L, log2S, mode == PM_DOUBLE ? "double" : "sandwich", ms[0], ms[1], ms[2],
+                         choice);
+            std::fclose(f);
+        }
+    }
+    std::lock_guard<std::mutex> lk(g_shape_mu);
+    g_shape[key] = choice;
+    return choice;
+}
+
 // Launch one fused axis pass: persistent grid (at most the resident CTAs), programmatic
 // dependent launch so the pass's prologue overlaps the tail of the previous kernel.
 static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
@@ -747,11 +841,12 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     // passes that reduce run the instantiation that carries the reduction code; the others keep its
     // registers for the transform
     int kmode = ps.mode;
-    if (ps.red.n && ps.mode == PM_DOUBLE && !ps.red_at_mid)
-        QND_FAIL(QND_EINVAL, "internal: a two-sandwich pass reduces between its sandwiches only");
     if (ps.red.n && ps.mode == PM_SANDWICH) kmode = PM_SANDWICH_RED;
     if (ps.red.n && ps.mode == PM_DOUBLE) kmode = PM_DOUBLE_RED;
-    const PassKernelInfo info = lookup_pass(c->fp64, L, strided, kmode);
+    // the shape variant: the default while recording (the sweep kernel holds the default shapes)
+    const int var = c->recorder ? 0 : (ps.force_shape >= 0 ? ps.force_shape : shape_choice(c, ps, L, log2S, kmode));
+    const PassKernelInfo info = lookup_pass(c->fp64, L, strided, kmode, var);
+    if (!info.fn) QND_FAIL(QND_EINVAL, "internal: no pass kernel for L=%d, mode %d, shape %d", L, kmode, var);
     const long long nlines = c->n / L;
     const long long ngroups = (nlines + info.G - 1) / info.G;
     if (c->recorder) {

@@ -14,8 +14,9 @@ struct PassKernelInfo {
     int E;        // values per thread (fixes the stage structure of the twiddle table)
 };
 
-// Defined once per line length in qnd_pass_inst.cu (compiled with -DQND_L=...).
-template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int mode);
+// Defined once per line length in qnd_pass_inst.cu (compiled with -DQND_L=...). var: the shape
+// variant (PassShape); fn is null where a variant does not exist.
+template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int mode, int var = 0);
 
 // Host-side copy of the FFTPlan stage structure for a runtime line length.
 struct HostPlan {

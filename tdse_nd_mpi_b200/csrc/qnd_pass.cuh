@@ -127,14 +127,22 @@ template <typename R> struct PassArgs {
 //   at L = 1024), else 16. T = L/E threads per line; a CTA of NT = T*G threads owns G lines.
 //   Lines along a strided axis are staged through shared memory with cp.async so that the
 //   global accesses run over G neighbouring lines; the stage buffer is then the exchange space.
-template <typename R, int L> struct PassShape {
+//
+// Shape variants VAR (the tile-shape autotuner picks one per geometry by timing, shape_choice in
+// qnd_engine.cu): 0 the default, 1 half the lines per CTA (smaller CTAs, more of them per SM),
+// 2 twice the lines per CTA (256-thread CTAs). Variants exist for the two-sandwich and sandwich
+// passes of lines of 256 to 2048 points; VALID says whether a variant differs from the default.
+constexpr int NSHAPES = 3;
+template <typename R, int L, int VAR = 0> struct PassShape {
     // FP64, L >= 1024: 32 values per thread (two radix-32 stages at L = 1024), one CTA per line, a
     // single warp per line at L = 1024 (warp-synchronous exchanges). Otherwise 16 values per thread
     // and 128-thread CTAs holding several lines.
     static constexpr bool WIDE = false;  // 32 values per thread for long FP64 lines: measured slower (too few warps per SM)
     static constexpr int E = L <= 16 ? L : (WIDE ? 32 : 16);
     static constexpr int T = L / E;
-    static constexpr int G = WIDE ? 1 : (T >= 128 ? 1 : 128 / T);
+    static constexpr int G0 = WIDE ? 1 : (T >= 128 ? 1 : 128 / T);
+    static constexpr int G = VAR == 1 ? (G0 > 1 ? G0 / 2 : 1) : (VAR == 2 ? 2 * G0 : G0);
+    static constexpr bool VALID = VAR == 0 || (L >= 256 && L <= 2048 && (VAR == 1 ? G0 > 1 : (T > 32 ? G <= 15 : true)));
     static constexpr int NT = T * G;
     static constexpr bool EXCHANGE = FFTPlan<L, E>::NSTAGE > 1;
     static constexpr int SLOTS = sizeof(R) == 8 ? 8 : 16;  // element slots per bank cycle (16 B / 8 B values)
@@ -153,7 +161,12 @@ template <typename R, int L> struct PassShape {
     static constexpr size_t SMEM = sizeof(cplx_t<R>) * (size_t(TWN) + size_t(G) * LS);
     // 128-thread CTAs: <= 128 registers (4 CTAs per SM) when shared memory allows; one-line CTAs
     // of L >= 1024 keep their registers (the SM holds as many lines as its register file allows)
-    static constexpr int MINB = WIDE ? 1 : (SMEM <= 54 * 1024 ? 4 : (SMEM <= 72 * 1024 ? 3 : (SMEM <= 110 * 1024 ? 2 : 1)));
+    static constexpr int MINB_DEFAULT =
+        WIDE ? 1 : (SMEM <= 54 * 1024 ? 4 : (SMEM <= 72 * 1024 ? 3 : (SMEM <= 110 * 1024 ? 2 : 1)));
+    // variants: as many CTAs as 128 registers a thread and the shared memory allow
+    static constexpr int MINB_REGS = 65536 / (NT * 128) > 0 ? 65536 / (NT * 128) : 1;
+    static constexpr int MINB_SMEM = int((227 * 1024) / (SMEM > 0 ? SMEM : 1)) > 0 ? int((227 * 1024) / (SMEM > 0 ? SMEM : 1)) : 1;
+    static constexpr int MINB = VAR == 0 ? MINB_DEFAULT : (MINB_REGS < MINB_SMEM ? MINB_REGS : MINB_SMEM);
 };
 
 // Barrier over the threads of one line: a named barrier when a line spans whole warps,
@@ -467,13 +480,13 @@ __device__ __forceinline__ void apply_factors(cplx_t<R>* v, int tid, long long b
 // memory smem_raw. `wait` runs after the prologue (twiddles to shared memory, read-only tables to
 // L2), before the state is touched: the wait for the previous pass (programmatic dependent launch
 // in qnd_pass_kernel, the pass's dependency counter in the persistent sweep kernel).
-template <typename R, int L, bool STRIDED, int KMODE, typename Wait>
+template <typename R, int L, bool STRIDED, int KMODE, int VAR = 0, typename Wait>
 __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, unsigned ngroups,
                                            unsigned char* smem_raw, Wait wait) {
     constexpr int MODE = pass_base_mode(KMODE);
     constexpr bool HAS_RED = pass_mode_reduces(KMODE);
     using V = cplx_t<R>;
-    using SH = PassShape<R, L>;
+    using SH = PassShape<R, L, VAR>;
     constexpr int E = SH::E, T = SH::T, G = SH::G, NT = SH::NT, LS = SH::LS;
     constexpr bool TWS = SH::TW_SMEM;
     V* tw_s = reinterpret_cast<V*>(smem_raw);   // [TWN] stage twiddles (when they fit)
@@ -657,7 +670,9 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
             else
                 apply_factors<R, E, T>(v, tid, base, lbase, nullptr, nullptr, nullptr, a.ax_real, a.axis, a.dim,
                                        a.shift, a.nmask, nullptr, key0 ^ 0x68e31da4u);
-            // (a two-sandwich pass reduces only between its sandwiches: red_at_mid, checked by the host)
+            // the end of a chain of 1-D sandwich pairs: reductions of the final state
+            if (HAS_RED && a.red.n && !a.red_at_mid)
+                accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);
         }
         store_out = true;
     } else {
@@ -742,15 +757,15 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
             for (int u = 0; u < E; ++u) out[base + tid + u * T] = v[u];
         }
     }
-    if constexpr (HAS_RED && MODE != PM_DOUBLE)
+    if constexpr (HAS_RED)
         if (MODE == PM_SPECRED || (a.red.n && !a.red_at_mid)) finish_red<NT>(a.red, acc, unsigned(g), ngroups);
 }
 
-template <typename R, int L, bool STRIDED, int KMODE>
-__global__ void __launch_bounds__(PassShape<R, L>::NT, PassShape<R, L>::MINB)
+template <typename R, int L, bool STRIDED, int KMODE, int VAR = 0>
+__global__ void __launch_bounds__(PassShape<R, L, VAR>::NT, PassShape<R, L, VAR>::MINB)
     qnd_pass_kernel(const __grid_constant__ PassArgs<R> a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    pass_group<R, L, STRIDED, KMODE>(a, blockIdx.x, gridDim.x, smem_raw, [] {
+    pass_group<R, L, STRIDED, KMODE, VAR>(a, blockIdx.x, gridDim.x, smem_raw, [] {
         pdl_wait();
         pdl_launch_dependents();
     });

@@ -8,7 +8,28 @@
 
 namespace qnd {
 
-template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int mode) {
+// A shape variant of the sandwich / two-sandwich passes (null where the variant is the default).
+template <typename R, int L, int VAR> static PassKernelInfo variant_info(bool strided, int mode) {
+    using SH = PassShape<R, L, VAR>;
+    const void* fn = nullptr;
+    if constexpr (SH::VALID) {
+#define QND_PICKV(M) \
+    (strided ? (const void*)&qnd_pass_kernel<R, L, true, M, VAR> : (const void*)&qnd_pass_kernel<R, L, false, M, VAR>)
+        switch (mode) {
+        case PM_SANDWICH: fn = QND_PICKV(PM_SANDWICH); break;
+        case PM_DOUBLE: fn = QND_PICKV(PM_DOUBLE); break;
+        case PM_SANDWICH_RED: fn = QND_PICKV(PM_SANDWICH_RED); break;
+        case PM_DOUBLE_RED: fn = QND_PICKV(PM_DOUBLE_RED); break;
+        default: fn = nullptr;
+        }
+#undef QND_PICKV
+    }
+    return PassKernelInfo{fn, SH::NT, SH::SMEM, SH::G, SH::TW_ENTRIES, SH::E};
+}
+
+template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int mode, int var) {
+    if (var == 1) return variant_info<R, L, 1>(strided, mode);
+    if (var == 2) return variant_info<R, L, 2>(strided, mode);
     using SH = PassShape<R, L>;
     const void* fn = nullptr;
 #define QND_PICK(M) \
@@ -29,7 +50,7 @@ template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int m
     return PassKernelInfo{fn, SH::NT, SH::SMEM, SH::G, SH::TW_ENTRIES, SH::E};
 }
 
-template PassKernelInfo pass_kernel_info<double, QND_L>(bool, int);
-template PassKernelInfo pass_kernel_info<float, QND_L>(bool, int);
+template PassKernelInfo pass_kernel_info<double, QND_L>(bool, int, int);
+template PassKernelInfo pass_kernel_info<float, QND_L>(bool, int, int);
 
 }  // namespace qnd

