@@ -81,7 +81,7 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
     objs = [obj for _, obj, _ in _jobs()]
     if force or todo or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
         tmp = LIB + ".tmp"
-        cmd = [nvcc, "-shared"] + ARCH + ["-o", tmp] + objs + ["-lcudart"]
+        cmd = [nvcc, "-shared"] + ARCH + ["-o", tmp] + objs + ["-lcudart", "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
