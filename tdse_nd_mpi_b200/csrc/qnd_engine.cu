@@ -3355,6 +3355,7 @@ int qnd_run_length_sweep(int count, qnd_ctx* const* ctxs, void* const* psi_r_dev
                 std::memcpy(blob.data() + nb, p.args.data(), p.args.size());
                 SweepSlot sl{};
                 sl.ngroups = p.ngroups;
+                sl.gpi = std::max(1u, p.ngroups / 64u);  // about 64 work items per pass
                 sl.need = need[i];
                 sl.member = i;
                 sl.L = p.L;
@@ -3363,7 +3364,7 @@ int qnd_run_length_sweep(int count, qnd_ctx* const* ctxs, void* const* psi_r_dev
                 slots.push_back(sl);
                 blob_off.push_back(nb);
                 first.push_back(nitems);
-                nitems += p.ngroups;
+                nitems += (p.ngroups + sl.gpi - 1) / sl.gpi;
                 need[i] += p.ngroups;
                 nb += argsz;
             }

@@ -165,13 +165,14 @@ constexpr int SWEEP_NT = 128;  // threads per CTA: every line length it takes ha
 struct SweepSlot {
     const void* args;
     unsigned ngroups;
-    unsigned need;
+    unsigned need;      // groups of the member's earlier passes that must be done before this one
+    unsigned gpi;       // line groups per work item (the last item of the pass may hold fewer)
     int member;
     int L, strided, kmode;
 };
 struct SweepArgs {
     const SweepSlot* slots;      // in round order: pass r of every member, member by member
-    const long long* first;      // [nslots] the first item (line group) of each slot
+    const long long* first;      // [nslots] the first work item of each slot
     int nslots;
     long long nitems;
     unsigned long long* next;    // item counter, zero at launch

@@ -4,7 +4,8 @@
 // Every member's run is a sequence of fused axis passes (its sandwich chains, recorded on the host
 // with the arguments the per-pass launches would get). A pass consists of line groups (a CTA's
 // share in qnd_pass_kernel); one group is one work item. The items are ordered by rounds: round r
-// holds pass r of every member that has one, member by member, group by group. Pass r of a member
+// holds pass r of every member that has one, member by member; a pass's items hold gpi groups each
+// (about 64 items per pass: fewer claims and waits per unit of work). Pass r of a member
 // needs all groups of its pass r - 1, which come earlier in that order, so a CTA that claims an item
 // (one atomic counter, in order) depends only on items already claimed by running CTAs: the launch
 // makes progress whenever its CTAs are all resident (a cooperative launch, sized by occupancy).
@@ -60,27 +61,50 @@ __device__ __forceinline__ void sweep_dispatch_stride(const SweepSlot& sl, long 
     else sweep_dispatch_mode<R, L, false>(sl, g, smem);
 }
 
+// The slot holding item, the last slot whose first item is <= item, searched forward from hint (the
+// slot of this CTA's previous item: items are claimed in increasing order) by doubling steps, then
+// bisection: a few loads where a search over all slots takes about fifteen dependent ones.
+__device__ __forceinline__ int sweep_slot_of(const SweepArgs& sa, long long item, int hint) {
+    int lo = hint, hi = sa.nslots - 1, step = 1;  // first[lo] <= item
+    for (;;) {
+        const int probe = lo + step;
+        if (probe >= sa.nslots) break;  // the answer is in [lo, nslots - 1]
+        if (sa.first[probe] <= item) {
+            lo = probe;
+            step <<= 1;
+        } else {
+            hi = probe - 1;  // the answer is in [lo, probe - 1]
+            break;
+        }
+    }
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sa.first[mid] <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 template <typename R>
 __global__ void __launch_bounds__(SWEEP_NT, 4) qnd_sweep_kernel(const __grid_constant__ SweepArgs sa) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ long long item_s;
-    __shared__ int go_s;
+    __shared__ int go_s, slot_s;
     const int t = threadIdx.x;
+    if (t == 0) slot_s = 0;
     for (;;) {
         __syncthreads();  // the previous item is done with the shared memory
-        if (t == 0) item_s = (long long)atomicAdd(sa.next, 1ull);
+        if (t == 0) {
+            const long long item = (long long)atomicAdd(sa.next, 1ull);
+            item_s = item;
+            if (item < sa.nitems) slot_s = sweep_slot_of(sa, item, slot_s);
+        }
         __syncthreads();
         const long long item = item_s;
         if (item >= sa.nitems) break;
-        // the slot of this item: the last slot whose first item is <= item
-        int lo = 0, hi = sa.nslots - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (sa.first[mid] <= item) lo = mid;
-            else hi = mid - 1;
-        }
-        const SweepSlot& sl = sa.slots[lo];
-        const long long g = item - sa.first[lo];
+        const SweepSlot& sl = sa.slots[slot_s];
+        const long long g0 = (item - sa.first[slot_s]) * sl.gpi;
+        const long long g1 = g0 + sl.gpi < (long long)sl.ngroups ? g0 + sl.gpi : (long long)sl.ngroups;
         if (t == 0) {
             bool ok = sweep_wait(sa.done + sl.member, sl.need, sa.abort_flag, sa.wait_tries);
             if (!ok) atomicExch(sa.abort_flag, 1);
@@ -88,18 +112,21 @@ __global__ void __launch_bounds__(SWEEP_NT, 4) qnd_sweep_kernel(const __grid_con
         }
         __syncthreads();
         if (go_s) {
-            switch (sl.L) {
-            case 128: sweep_dispatch_stride<R, 128>(sl, g, smem); break;
-            case 256: sweep_dispatch_stride<R, 256>(sl, g, smem); break;
-            case 512: sweep_dispatch_stride<R, 512>(sl, g, smem); break;
-            case 1024: sweep_dispatch_stride<R, 1024>(sl, g, smem); break;
-            default: break;  // the host records only these lengths
+            for (long long g = g0; g < g1; ++g) {
+                if (g > g0) __syncthreads();  // the previous group is done with the shared memory
+                switch (sl.L) {
+                case 128: sweep_dispatch_stride<R, 128>(sl, g, smem); break;
+                case 256: sweep_dispatch_stride<R, 256>(sl, g, smem); break;
+                case 512: sweep_dispatch_stride<R, 512>(sl, g, smem); break;
+                case 1024: sweep_dispatch_stride<R, 1024>(sl, g, smem); break;
+                default: break;  // the host records only these lengths
+                }
             }
         }
-        __syncthreads();  // every store of the group issued
+        __syncthreads();  // every store of the item issued
         if (t == 0) {
             __threadfence();
-            atomicAdd(sa.done + sl.member, 1u);
+            atomicAdd(sa.done + sl.member, unsigned(g1 - g0));
         }
     }
 }
