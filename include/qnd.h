@@ -51,8 +51,8 @@ const char *qnd_last_error(void);
 /* ---- context: replaces Initialize_meshgrid (meshgrid.c:17-179) and
  *      Initialize_integrator (integrators.c:13-71). dim is 1 to 6 (the reference takes any
  *      DIMENSION, parameters.c:46-48). nr[j] must be a power of two
- *      (parameters.c:72-76) between 2 and 4096, or up to 2^24 on a 1-D grid (QND_EUNSUPPORTED
- *      beyond). integrator: Verlet, BM4, BM6, RKN4. */
+ *      (parameters.c:72-76) between 2 and 2^24 (QND_EUNSUPPORTED beyond); axes longer than
+ *      4096 points take a four-step transform. integrator: Verlet, BM4, BM6, RKN4. */
 int qnd_ctx_create(int dim, const int64_t *nr, const double *dr, const char *integrator, double dt, int precision,
                    qnd_ctx **out);
 int qnd_ctx_destroy(qnd_ctx *ctx);

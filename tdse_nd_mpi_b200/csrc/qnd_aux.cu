@@ -415,6 +415,64 @@ __global__ void __launch_bounds__(256) add_potential_kernel(long long n, cplx_t<
         dst[i] = cadd(dst[i], cscale(src[i], R(vtab[i])));
 }
 
+template <typename R>
+__global__ void __launch_bounds__(256) axis_factors_kernel(const __grid_constant__ AxisFactorArgs a, cplx_t<R>* psi) {
+    using V = cplx_t<R>;
+    const int sa = a.shift[a.axis];
+    const long long smask = (1ll << sa) - 1;
+    const R sc = a.scale_dev ? R(*a.scale_dev) : R(1);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (long long)gridDim.x * blockDim.x) {
+        const long long q = (i >> sa) & a.nmask[a.axis];
+        V x = psi[i];
+        if (a.tr || a.tc) {
+            const long long lam = ((i >> (sa + a.log2L)) << sa) | (i & smask);
+            const long long lm = (lam << a.log2L) + q;
+            if (a.tr) x = cscale(x, static_cast<const R*>(a.tr)[lm]);
+            if (a.tc) x = fmul(x, static_cast<const V*>(a.tc)[lm]);
+        }
+        for (int k = 0; k < a.dim; ++k) {
+            const long long ik = (i >> a.shift[k]) & a.nmask[k];
+            if (a.axc[k]) x = fmul(x, static_cast<const V*>(a.axc[k])[ik]);
+            if (a.axr[k]) x = cscale(x, static_cast<const R*>(a.axr[k])[ik]);
+        }
+        if (a.spec) {
+            V f = static_cast<const V*>(a.spec)[q];
+            if (a.spec_conj) f.y = -f.y;  // conj(w), and for FP32 tables conj(w - 1) = conj(w) - 1
+            x = fmul(x, f);
+            if (a.spec_scale != 1.0) x = cscale(x, R(a.spec_scale));
+        }
+        if (a.scale_dev) x = cscale(x, sc);
+        psi[i] = x;
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) axis_permute_kernel(AxisPermArgs a, const cplx_t<R>* in, cplx_t<R>* out,
+                                                           int to_natural) {
+    const long long nm = (1ll << a.log2N) - 1;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (long long)gridDim.x * blockDim.x) {
+        const long long q = (i >> a.shift) & nm;
+        long long src;
+        if (to_natural) {  // q is the frequency k1 + n1 k2, held at slot k1 n2 + k2
+            src = ((q & ((1ll << a.log2n1) - 1)) << a.log2n2) + (q >> a.log2n1);
+        } else {           // q is the slot k1 n2 + k2, holding frequency k1 + n1 k2
+            src = (q >> a.log2n2) + ((q & ((1ll << a.log2n2) - 1)) << a.log2n1);
+        }
+        out[i] = in[i + (src - q) * (1ll << a.shift)];
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) apply_combine_kernel(long long n, cplx_t<R>* dst, const cplx_t<R>* tmp,
+                                                            const cplx_t<R>* src, const double* vtab, int acc) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        cplx_t<R> x = tmp[i];
+        if (vtab) x = cadd(x, cscale(src[i], R(vtab[i])));
+        if (acc) x = cadd(x, dst[i]);
+        dst[i] = x;
+    }
+}
+
 struct MaskArgs {
     int dim;
     int shift[MAX_DIM];
@@ -466,6 +524,18 @@ template <typename R> void launch_add_potential(long long n, cplx_t<R>* dst, con
     add_potential_kernel<R><<<elementwise_blocks(n), 256, 0, st>>>(n, dst, src, vtab);
 }
 
+template <typename R> void launch_axis_factors(const AxisFactorArgs& a, cplx_t<R>* psi, cudaStream_t st) {
+    axis_factors_kernel<R><<<elementwise_blocks(a.n), 256, 0, st>>>(a, psi);
+}
+template <typename R> void launch_axis_permute(const AxisPermArgs& a, const cplx_t<R>* in, cplx_t<R>* out,
+                                               int to_natural, cudaStream_t st) {
+    axis_permute_kernel<R><<<elementwise_blocks(a.n), 256, 0, st>>>(a, in, out, to_natural);
+}
+template <typename R> void launch_apply_combine(long long n, cplx_t<R>* dst, const cplx_t<R>* tmp,
+                                               const cplx_t<R>* src, const double* vtab, int acc, cudaStream_t st) {
+    apply_combine_kernel<R><<<elementwise_blocks(n), 256, 0, st>>>(n, dst, tmp, src, vtab, acc);
+}
+
 #define QND_INST(R)                                                                               \
     template void launch_gs_dot<R>(const GSArgs<R>&, cudaStream_t, int);                          \
     template void launch_gs_axpy<R>(const GSArgs<R>&, cudaStream_t, int);                         \
@@ -483,7 +553,11 @@ template <typename R> void launch_add_potential(long long n, cplx_t<R>* dst, con
     template void launch_add_potential<R>(long long, cplx_t<R>*, const cplx_t<R>*, const double*, cudaStream_t); \
     template void launch_embed<R>(const EmbedArgs&, const double2*, cplx_t<R>*, cudaStream_t);                \
     template void launch_apply_masks<R>(long long, cplx_t<R>*, int, const int*, const long long*, const R* const*, \
-                                        cudaStream_t);
+                                        cudaStream_t);                                                      \
+    template void launch_axis_factors<R>(const AxisFactorArgs&, cplx_t<R>*, cudaStream_t);                   \
+    template void launch_axis_permute<R>(const AxisPermArgs&, const cplx_t<R>*, cplx_t<R>*, int, cudaStream_t); \
+    template void launch_apply_combine<R>(long long, cplx_t<R>*, const cplx_t<R>*, const cplx_t<R>*, const double*, \
+                                          int, cudaStream_t);
 QND_INST(double)
 QND_INST(float)
 #undef QND_INST

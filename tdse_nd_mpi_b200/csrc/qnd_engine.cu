@@ -202,6 +202,16 @@ struct qnd_ctx {
     int64_t n1 = 0, n2 = 0;
     int lg1 = 0, lg2 = 0;
     DevBuf tw_long[2], twf_long, twc_long, p_slot_dev, long_tmp;
+    // Axes longer than 4096 points on grids of several dimensions (emulate_long_pass): per axis the
+    // virtual lengths n1 n2, their pass twiddles, the four-step twiddles and their conjugates (at
+    // slot k1 n2 + m, as for the 1-D long axis); two scratch states for permutations and copies.
+    struct LongAxis {
+        bool on = false;
+        int64_t n1 = 0, n2 = 0;
+        int lg1 = 0, lg2 = 0;
+        DevBuf tw[2], twf, twc;
+    } lax[MAX_DIM];
+    DevBuf lax_perm, lax_tmp;
     std::vector<double> p_slot;
     std::vector<char> host_tmp;
 
@@ -886,10 +896,19 @@ static int shape_choice(qnd_ctx* c, const PassSpec& ps, int L, int log2S, int km
     return choice;
 }
 
+static void emulate_long_pass(qnd_ctx* c, const PassSpec& ps);
+
 // Launch one fused axis pass: persistent grid (at most the resident CTAs), programmatic
 // dependent launch so the pass's prologue overlaps the tail of the previous kernel.
 static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     const int ax = ps.axis;
+    if (!ps.vL && c->lax[ax].on) {
+        if (c->recorder)
+            QND_FAIL(QND_EUNSUPPORTED, "qnd_run_length_sweep: an axis of %lld points is outside the sweep kernel "
+                                       "(axis lengths 128 to 1024)", (long long)c->nr[ax]);
+        emulate_long_pass(c, ps);  // an axis longer than one pass holds (several dimensions)
+        return;
+    }
     const int L = ps.vL ? ps.vL : int(c->nr[ax]);
     const int log2S = ps.vL ? ps.vlog2S : c->shift[ax];
     const void* tw = ps.vL ? ps.vtw : c->tw[ax].p;
@@ -1026,7 +1045,9 @@ static int reduce_blocks(qnd_ctx* c) {
 }
 
 // Element-wise r-space reductions of psi.
-static void grid_reduce(qnd_ctx* c, const void* psi, const RedDesc& rd_in, const void* partner = nullptr) {
+// lm_axis >= 0: the full-grid weights are in the line-major order of that axis (a pass's layout).
+static void grid_reduce(qnd_ctx* c, const void* psi, const RedDesc& rd_in, const void* partner = nullptr,
+                        int lm_axis = -1) {
     RedDesc rd = rd_in;
     const int nb = reduce_blocks(c);
     ensure_red_scratch(c, nb);
@@ -1036,13 +1057,16 @@ static void grid_reduce(qnd_ctx* c, const void* psi, const RedDesc& rd_in, const
     ps.psi = const_cast<void*>(psi);
     ps.partner = partner;
     ps.red = rd;
+    ps.axis = lm_axis >= 0 ? lm_axis : 0;
     if (c->fp64) {
         PassArgs<double> a;
         fill_args<double>(c, ps, a);
+        a.red_lm = lm_axis >= 0;
         launch_grid_reduce<double>(a, c->n, c->stream, nb);
     } else {
         PassArgs<float> a;
         fill_args<float>(c, ps, a);
+        a.red_lm = lm_axis >= 0;
         launch_grid_reduce<float>(a, c->n, c->stream, nb);
     }
     c->kernels_launched++;
@@ -1077,6 +1101,164 @@ static std::vector<int> pass_order(const qnd_ctx* c) {
     std::vector<int> o;
     for (int k = c->dim - 1; k >= 0; --k) o.push_back(k);
     return o;
+}
+
+// ---------------------------------------------------------------- long axes of N-D grids --
+//
+// On a grid of two or more dimensions, an axis j of N > 4096 points (N = n1 n2) is transformed in
+// four steps in natural order: the length-n1 pass along the virtual axis of stride n2 S_j, the
+// twiddles W_N^{k1 m} (element-wise along j), the length-n2 pass along the virtual axis of stride
+// S_j, and a permutation from the slot order (slot k1 n2 + k2 holds frequency k1 + n1 k2) to
+// natural order; the inverse runs the other way. A pass along j (any mode) is then emulated from
+// these transforms and element-wise kernels that apply its factors in natural order (its full-grid
+// tables are read in their line-major order for j) and reduce it. Every operation built on passes
+// (sandwich chains, imaginary time, the velocity gauge, k-space observables, spectra, adjoints)
+// takes such axes unchanged; the cost is more launches and memory passes than a fused pass.
+
+static PassSpec lax_pass(qnd_ctx* c, int ax, int v, int mode, void* psi, double scale) {
+    const auto& la = c->lax[ax];
+    PassSpec ps;
+    ps.axis = ax;
+    ps.mode = mode;
+    ps.psi = psi;
+    ps.scale = scale;
+    ps.vL = int(v == 0 ? la.n1 : la.n2);
+    ps.vlog2S = v == 0 ? la.lg2 + c->shift[ax] : c->shift[ax];
+    ps.vtw = la.tw[v].p;
+    return ps;
+}
+
+// Element-wise factors along axis ax (see AxisFactorArgs); any pointer may be null.
+static void lax_factors(qnd_ctx* c, void* psi, int ax, const void* tr, const void* tc, const void* const* axc,
+                        const void* const* axr, const void* spec, int spec_conj, double spec_scale,
+                        const double* scale_dev) {
+    if (!tr && !tc && !spec && !scale_dev) {
+        bool any = false;
+        for (int k = 0; k < c->dim; ++k) any = any || (axc && axc[k]) || (axr && axr[k]);
+        if (!any) return;
+    }
+    AxisFactorArgs a{};
+    a.n = c->n;
+    a.dim = c->dim;
+    a.axis = ax;
+    a.log2L = c->lognr[ax];
+    for (int k = 0; k < MAX_DIM; ++k) {
+        a.shift[k] = c->shift[k];
+        a.nmask[k] = c->nr[k] - 1;
+        a.axc[k] = axc ? axc[k] : nullptr;
+        a.axr[k] = axr ? axr[k] : nullptr;
+    }
+    a.tr = tr;
+    a.tc = tc;
+    a.spec = spec;
+    a.spec_conj = spec_conj;
+    a.spec_scale = spec_scale;
+    a.scale_dev = scale_dev;
+    if (c->fp64) launch_axis_factors<double>(a, static_cast<double2*>(psi), c->stream);
+    else launch_axis_factors<float>(a, static_cast<float2*>(psi), c->stream);
+    c->kernels_launched++;
+    QND_CK(cudaGetLastError());
+}
+
+static void lax_permute(qnd_ctx* c, void* psi, int ax, bool to_natural) {
+    const auto& la = c->lax[ax];
+    c->lax_perm.ensure(size_t(c->n) * c->elem());
+    AxisPermArgs a{};
+    a.n = c->n;
+    a.shift = c->shift[ax];
+    a.log2N = c->lognr[ax];
+    a.log2n1 = la.lg1;
+    a.log2n2 = la.lg2;
+    if (c->fp64)
+        launch_axis_permute<double>(a, static_cast<const double2*>(psi), c->lax_perm.as<double2>(), to_natural, c->stream);
+    else
+        launch_axis_permute<float>(a, static_cast<const float2*>(psi), c->lax_perm.as<float2>(), to_natural, c->stream);
+    c->kernels_launched++;
+    QND_CK(cudaGetLastError());
+    QND_CK(cudaMemcpyAsync(psi, c->lax_perm.p, size_t(c->n) * c->elem(), cudaMemcpyDeviceToDevice, c->stream));
+}
+
+// Unnormalised transform along axis ax (times scale), natural order in and out.
+static void lax_fft(qnd_ctx* c, void* psi, int ax, bool forward, double scale) {
+    const auto& la = c->lax[ax];
+    if (forward) {
+        launch_pass(c, lax_pass(c, ax, 0, PM_FFT_FWD, psi, 1.0));
+        lax_factors(c, psi, ax, nullptr, nullptr, nullptr, nullptr, la.twf.p, 0, 1.0, nullptr);
+        launch_pass(c, lax_pass(c, ax, 1, PM_FFT_FWD, psi, scale));
+        lax_permute(c, psi, ax, true);
+    } else {
+        lax_permute(c, psi, ax, false);
+        launch_pass(c, lax_pass(c, ax, 1, PM_FFT_INV, psi, 1.0));
+        lax_factors(c, psi, ax, nullptr, nullptr, nullptr, nullptr, la.twc.p, 0, 1.0, nullptr);
+        launch_pass(c, lax_pass(c, ax, 0, PM_FFT_INV, psi, scale));
+    }
+}
+
+static void emulate_long_pass(qnd_ctx* c, const PassSpec& ps) {
+    const int ax = ps.axis;
+    const int mode = ps.mode;
+    if (ps.spec_full) QND_FAIL(QND_EINVAL, "internal: a full-grid spectral table along a long axis");
+    // FP32 spectral tables hold d = w N_axis - 1; the 1/N_axis is applied as a scaling
+    const double sscale = c->fp64 ? 1.0 : 1.0 / double(c->nr[ax]);
+    void* psi = ps.psi;
+    auto sandwich = [&](void* buf, const void* spec) {
+        lax_fft(c, buf, ax, true, 1.0);
+        lax_factors(c, buf, ax, nullptr, nullptr, nullptr, nullptr, spec, 0, spec ? sscale : 1.0, nullptr);
+        lax_fft(c, buf, ax, false, 1.0);
+    };
+    auto reduce = [&](const void* buf) {
+        if (ps.red.n) grid_reduce(c, buf, ps.red, ps.partner, ax);
+    };
+    if (mode == PM_FFT_FWD || mode == PM_FFT_INV) {
+        lax_fft(c, psi, ax, mode == PM_FFT_FWD, ps.scale);
+        return;
+    }
+    if (mode == PM_SANDWICH || mode == PM_DOUBLE) {
+        lax_factors(c, psi, ax, ps.pro_real, ps.pro_cplx, ps.ax_in_prologue ? ps.ax_cplx : nullptr, nullptr, nullptr, 0,
+                    1.0, ps.pro_scale);
+        sandwich(psi, ps.spec);
+        if (mode == PM_DOUBLE) {
+            lax_factors(c, psi, ax, ps.mid_real, ps.mid_cplx, ps.mid_ax_cplx, ps.mid_ax_real, nullptr, 0, 1.0, nullptr);
+            if (ps.red_at_mid) reduce(psi);
+            sandwich(psi, ps.spec2);
+        }
+        lax_factors(c, psi, ax, ps.epi_real, ps.epi_cplx, ps.ax_in_prologue ? nullptr : ps.ax_cplx, ps.ax_real, nullptr, 0,
+                    1.0, nullptr);
+        if (!ps.red_at_mid) reduce(psi);
+        return;
+    }
+    if (mode == PM_APPLY || mode == PM_SPECRED) {
+        // on a copy: the pass's state is not modified
+        c->lax_tmp.ensure(size_t(c->n) * c->elem());
+        void* tmp = c->lax_tmp.p;
+        QND_CK(cudaMemcpyAsync(tmp, psi, size_t(c->n) * c->elem(), cudaMemcpyDeviceToDevice, c->stream));
+        if (mode == PM_SPECRED) {
+            lax_fft(c, tmp, ax, true, 1.0);
+            reduce(tmp);
+            return;
+        }
+        sandwich(tmp, ps.spec);
+        if (ps.apply_vtab || ps.apply_acc) {
+            if (ps.apply_acc && !ps.dst) QND_FAIL(QND_EINVAL, "internal: an accumulating apply pass without dst");
+            void* out = ps.apply_acc ? ps.dst : tmp;
+            if (c->fp64)
+                launch_apply_combine<double>(c->n, static_cast<double2*>(out), static_cast<const double2*>(tmp),
+                                             static_cast<const double2*>(psi), ps.apply_vtab, ps.apply_acc, c->stream);
+            else
+                launch_apply_combine<float>(c->n, static_cast<float2*>(out), static_cast<const float2*>(tmp),
+                                            static_cast<const float2*>(psi), ps.apply_vtab, ps.apply_acc, c->stream);
+            c->kernels_launched++;
+            QND_CK(cudaGetLastError());
+            if (ps.apply_acc) {
+                reduce(ps.dst);
+                return;
+            }
+        }
+        if (ps.dst) QND_CK(cudaMemcpyAsync(ps.dst, tmp, size_t(c->n) * c->elem(), cudaMemcpyDeviceToDevice, c->stream));
+        reduce(ps.dst ? ps.dst : tmp);
+        return;
+    }
+    QND_FAIL(QND_EUNSUPPORTED, "internal: pass mode %d along an axis longer than 4096 points", mode);
 }
 
 // ---------------------------------------------------------------- long axes --
@@ -2295,22 +2477,14 @@ static void scale_state(qnd_ctx* c, void* psi, const double* scale_dev) {
 
 static void set_device(qnd_ctx* c) { QND_CK(cudaSetDevice(c->device)); }
 
-// The tables of a long 1-D axis (see long_fft): pass twiddles for both virtual lengths, the
-// four-step twiddles W_N^{k1 n2} and their conjugates (FP32: stored as w - 1), slot momenta.
-static void build_long_axis(qnd_ctx* c) {
-    const int64_t N = c->nr[0];
-    c->long1d = true;
-    c->lg1 = std::max(4, c->lognr[0] - 12);  // n1 >= 16: the strided passes keep 16 values per thread
-    c->lg2 = c->lognr[0] - c->lg1;
-    c->n1 = int64_t(1) << c->lg1;
-    c->n2 = int64_t(1) << c->lg2;
-    build_twiddles(c, int(c->n1), c->tw_long[0]);
-    build_twiddles(c, int(c->n2), c->tw_long[1]);
+// The four-step twiddles of an axis of N = n1 n2 points: W_N^{k1 m} at slot k1 n2 + m, and their
+// conjugates (FP32: stored as w - 1).
+static void build_four_step_twiddles(qnd_ctx* c, int64_t N, int64_t n1, int64_t n2, DevBuf& twf, DevBuf& twc) {
     std::vector<double> w(2 * size_t(N)), wc(2 * size_t(N));
     const long double two_pi = 6.283185307179586476925286766559005768L;
-    for (int64_t k1 = 0; k1 < c->n1; ++k1)
-        for (int64_t m = 0; m < c->n2; ++m) {
-            const int64_t i = k1 * c->n2 + m;
+    for (int64_t k1 = 0; k1 < n1; ++k1)
+        for (int64_t m = 0; m < n2; ++m) {
+            const int64_t i = k1 * n2 + m;
             const long double ang = two_pi * (long double)((k1 * m) & (N - 1)) / (long double)N;
             const double sn = (double)sinl(ang);
             double re;
@@ -2325,8 +2499,37 @@ static void build_long_axis(qnd_ctx* c) {
             wc[2 * i] = re;
             wc[2 * i + 1] = sn;
         }
-    upload_cplx(c, c->twf_long, w);
-    upload_cplx(c, c->twc_long, wc);
+    upload_cplx(c, twf, w);
+    upload_cplx(c, twc, wc);
+}
+
+// An axis longer than 4096 points on a grid of several dimensions (emulate_long_pass): the virtual
+// lengths (n2 = min(4096, N / 16), n1 = N / n2), their pass twiddles, the four-step twiddles.
+static void build_long_axis_nd(qnd_ctx* c, int ax) {
+    auto& la = c->lax[ax];
+    const int64_t N = c->nr[ax];
+    la.on = true;
+    la.lg1 = std::max(4, c->lognr[ax] - 12);
+    la.lg2 = c->lognr[ax] - la.lg1;
+    la.n1 = int64_t(1) << la.lg1;
+    la.n2 = int64_t(1) << la.lg2;
+    build_twiddles(c, int(la.n1), la.tw[0]);
+    build_twiddles(c, int(la.n2), la.tw[1]);
+    build_four_step_twiddles(c, N, la.n1, la.n2, la.twf, la.twc);
+}
+
+// The tables of a long 1-D axis (see long_fft): pass twiddles for both virtual lengths, the
+// four-step twiddles W_N^{k1 n2} and their conjugates (FP32: stored as w - 1), slot momenta.
+static void build_long_axis(qnd_ctx* c) {
+    const int64_t N = c->nr[0];
+    c->long1d = true;
+    c->lg1 = std::max(4, c->lognr[0] - 12);  // n1 >= 16: the strided passes keep 16 values per thread
+    c->lg2 = c->lognr[0] - c->lg1;
+    c->n1 = int64_t(1) << c->lg1;
+    c->n2 = int64_t(1) << c->lg2;
+    build_twiddles(c, int(c->n1), c->tw_long[0]);
+    build_twiddles(c, int(c->n2), c->tw_long[1]);
+    build_four_step_twiddles(c, N, c->n1, c->n2, c->twf_long, c->twc_long);
     c->p_slot.resize(size_t(N));
     for (int64_t i = 0; i < N; ++i) c->p_slot[i] = c->p[0][(i >> c->lg2) + ((i & (c->n2 - 1)) << c->lg1)];
     upload_f64(c, c->p_slot_dev, c->p_slot);
@@ -2339,13 +2542,12 @@ static void build_context(qnd_ctx* c, int dim, const int64_t* nr, const double* 
     c->fp64 = precision == QND_FP64;
     c->dim = dim;
     c->n = 1;
-    // one pass handles an axis of up to 4096 points; a 1-D grid goes up to 2^24 points in four steps
-    const int64_t nmax = dim == 1 ? LONG_AXIS_MAX : 4096;
+    // one pass handles an axis of up to 4096 points; longer axes (up to 2^24 points) take four steps
+    const int64_t nmax = LONG_AXIS_MAX;
     for (int j = 0; j < dim; ++j) {
         if (nr[j] < 2 || nr[j] > nmax || (nr[j] & (nr[j] - 1)))
             QND_FAIL(nr[j] > nmax ? QND_EUNSUPPORTED : QND_EINVAL,
-                     "NR[%d]=%lld: must be a power of 2 between 2 and %lld%s", j, (long long)nr[j], (long long)nmax,
-                     dim == 1 ? "" : " (axes longer than 4096 are built for 1-D grids)");
+                     "NR[%d]=%lld: must be a power of 2 between 2 and %lld", j, (long long)nr[j], (long long)nmax);
         if (!(dr[j] > 0)) QND_FAIL(QND_EINVAL, "DR[%d] must be positive", j);
         c->nr[j] = nr[j];
         c->dr[j] = dr[j];
@@ -2418,7 +2620,20 @@ static void build_context(qnd_ctx* c, int dim, const int64_t* nr, const double* 
         build_long_axis(c);
         return;
     }
-    for (int j = 0; j < dim; ++j) build_twiddles(c, int(c->nr[j]), c->tw[j]);
+    bool any_long = false;
+    for (int j = 0; j < dim; ++j) {
+        if (c->nr[j] > 4096) {
+            build_long_axis_nd(c, j);
+            any_long = true;
+        } else {
+            build_twiddles(c, int(c->nr[j]), c->tw[j]);
+        }
+    }
+    if (any_long) {
+        // the scratch states of the emulated passes, allocated up front (not inside a graph capture)
+        c->lax_perm.ensure(size_t(c->n) * c->elem());
+        c->lax_tmp.ensure(size_t(c->n) * c->elem());
+    }
 }
 
 // Named potentials as functions of |r| (meshgrid.c:137-153) and their radial derivative dV/dr.

@@ -158,6 +158,38 @@ template <typename R> void launch_apply_masks(long long n, cplx_t<R>* psi, int d
 template <typename R> void launch_add_potential(long long n, cplx_t<R>* dst, const cplx_t<R>* src, const double* vtab,
                                                 cudaStream_t st);
 
+// ---- passes along an axis longer than one pass holds, on a grid of several dimensions
+// (emulate_long_pass in qnd_engine.cu): element-wise work along that axis in natural order.
+// psi *= tr[lm] * tc[lm] * prod_k axc[k][i_k] * prod_k axr[k][i_k] * spec[i_axis] * spec_scale * *scale_dev,
+// every table optional; lm is the element's index in the line-major order of the axis (the layout of
+// the pass's full-grid tables), i_k its index along axis k.
+struct AxisFactorArgs {
+    long long n;
+    int dim, axis, log2L;
+    int shift[MAX_DIM];
+    long long nmask[MAX_DIM];
+    const void* tr;
+    const void* tc;
+    const void* axc[MAX_DIM];
+    const void* axr[MAX_DIM];
+    const void* spec;
+    int spec_conj;
+    double spec_scale;
+    const double* scale_dev;
+};
+template <typename R> void launch_axis_factors(const AxisFactorArgs& a, cplx_t<R>* psi, cudaStream_t st);
+// The four-step order along an axis of N = n1 n2 points at stride 2^shift (slot k1 n2 + k2 holds
+// frequency k1 + n1 k2): out = in reordered to natural order (to_natural) or back to slot order.
+struct AxisPermArgs {
+    long long n;
+    int shift, log2N, log2n1, log2n2;
+};
+template <typename R> void launch_axis_permute(const AxisPermArgs& a, const cplx_t<R>* in, cplx_t<R>* out,
+                                               int to_natural, cudaStream_t st);
+// dst = tmp + vtab * src (vtab may be null) + dst (when acc)
+template <typename R> void launch_apply_combine(long long n, cplx_t<R>* dst, const cplx_t<R>* tmp,
+                                               const cplx_t<R>* src, const double* vtab, int acc, cudaStream_t st);
+
 // ---- the persistent sweep kernel (qnd_sweep.cu): recorded passes of many members in one launch
 constexpr int SWEEP_NT = 128;  // threads per CTA: every line length it takes has 128-thread pass CTAs
 // One recorded pass of one member: its arguments (PassArgs<R> in device memory), its line groups,

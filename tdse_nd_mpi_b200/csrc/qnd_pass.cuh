@@ -119,6 +119,7 @@ template <typename R> struct PassArgs {
     int use_tma;
     int* err;
     int tma_wait_tries;          // tries of the bounded wait for those loads before the CTA gives up
+    int red_lm;                  // grid reductions: full-grid weights in the line-major order of `axis`
     CUtensorMap tmap;
 };
 
@@ -779,8 +780,16 @@ __global__ void __launch_bounds__(256) qnd_grid_reduce_kernel(const __grid_const
     double acc[MAX_RED];
 #pragma unroll
     for (int k = 0; k < MAX_RED; ++k) acc[k] = 0.0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        accumulate_red<R>(a.red, acc, a.psi[i], a.partner, i, i, a.shift, a.nmask);
+    const int sa = a.shift[a.axis];
+    const long long L = a.nmask[a.axis] + 1;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        long long li = i;  // the index of element i in the weights' order
+        if (a.red_lm) {
+            const long long q = (i >> sa) & a.nmask[a.axis];
+            li = ((((i >> sa) / L) << sa) | (i & ((1ll << sa) - 1))) * L + q;
+        }
+        accumulate_red<R>(a.red, acc, a.psi[i], a.partner, i, li, a.shift, a.nmask);
+    }
     finish_red<256>(a.red, acc);
 }
 

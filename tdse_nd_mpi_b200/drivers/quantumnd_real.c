@@ -8,8 +8,7 @@
  *
  *     QuantumND_real <params.real> [KEY VALUE ...]
  *
- * Grids are limited to what the engine builds: powers of two up to 4096 per axis, and up to 2^24
- * points on a 1-D grid.
+ * Grids are limited to what the engine builds: powers of two up to 2^24 points per axis.
  */
 #include <complex.h>
 #include <math.h>

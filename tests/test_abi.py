@@ -44,7 +44,7 @@ def _create(dim, nr, dr, integ="BM4", dt=0.05, prec=0):
     [
         ((1, (100,), (0.1,)), _lib.QND_EINVAL),            # not a power of two (parameters.c:72-76)
         ((1, (1 << 25,), (0.1,)), _lib.QND_EUNSUPPORTED),  # beyond the longest 1-D axis (2^24)
-        ((2, (8192, 8), (0.1, 0.1)), _lib.QND_EUNSUPPORTED),  # axes > 4096 are built for 1-D grids only
+        ((2, (1 << 25, 2), (0.1, 0.1)), _lib.QND_EUNSUPPORTED),  # beyond the longest axis (2^24)
         ((7, (2,) * 7, (1,) * 7), _lib.QND_EINVAL),        # beyond the 6 dimensions built
         ((1, (64,), (-0.1,)), _lib.QND_EINVAL),
     ],
