@@ -3570,10 +3570,9 @@ int qnd_run_length_sweep(int count, qnd_ctx* const* ctxs, void* const* psi_r_dev
                 std::memcpy(blob.data() + nb, p.args.data(), p.args.size());
                 SweepSlot sl{};
                 sl.ngroups = p.ngroups;
-                // work items of about 16384 points (the groups of one item run back to back in one
-                // CTA): fewer claims and waits for the small members' passes
-                const long long ppg = (ms[i].c->n + p.ngroups - 1) / p.ngroups;
-                sl.gpi = unsigned(std::min<long long>(p.ngroups, std::max<long long>(1, 16384 / std::max(1ll, ppg))));
+                // about 64 work items per pass (measured: items of a fixed size of about 16384 points,
+                // fewer for the small members' passes, ran the 96-member sweep 10% slower)
+                sl.gpi = std::max(1u, p.ngroups / 64u);
                 sl.need = need[i];
                 sl.member = i;
                 sl.L = p.L;

@@ -5,7 +5,7 @@
 // with the arguments the per-pass launches would get). A pass consists of line groups (a CTA's
 // share in qnd_pass_kernel); one group is one work item. The items are ordered by rounds: round r
 // holds pass r of every member that has one, member by member; a pass's items hold gpi groups each
-// (about 16384 points per item: fewer claims and waits per unit of work). Pass r of a member
+// (about 64 items per pass: fewer claims and waits per unit of work). Pass r of a member
 // needs all groups of its pass r - 1, which come earlier in that order, so a CTA that claims an item
 // (one atomic counter, in order) depends only on items already claimed by running CTAs: the launch
 // makes progress whenever its CTAs are all resident (a cooperative launch, sized by occupancy).
