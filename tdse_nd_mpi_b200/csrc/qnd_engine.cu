@@ -579,6 +579,15 @@ static int tma_wait_tries() {
     return v < 0 ? 0 : (v > (1 << 20) ? (1 << 20) : int(v));
 }
 
+// The log2 stride and index mask of each axis-weighted reduction's axis (RedDesc wshift / wmask).
+static void set_red_axes(const qnd_ctx* c, RedDesc& rd) {
+    for (int k = 0; k < rd.n && k < MAX_RED; ++k) {
+        const int wax = rd.waxis[k] >= 0 && rd.waxis[k] < c->dim ? rd.waxis[k] : 0;
+        rd.wshift[k] = c->shift[wax];
+        rd.wmask[k] = c->nr[wax] - 1;
+    }
+}
+
 template <typename R> static void fill_args(qnd_ctx* c, const PassSpec& ps, PassArgs<R>& a) {
     using V = cplx_t<R>;
     std::memset(&a, 0, sizeof a);
@@ -616,6 +625,7 @@ template <typename R> static void fill_args(qnd_ctx* c, const PassSpec& ps, Pass
     a.apply_vtab = ps.apply_vtab;
     a.seed = uint32_t(c->kernels_launched) * 0x9e3779b9u + 0x632be5abu;
     a.red = ps.red;
+    set_red_axes(c, a.red);
     a.err = c->err_flag.as<int>();
     a.tma_wait_tries = tma_wait_tries();
 }
@@ -761,7 +771,8 @@ static void check_device_error(qnd_ctx* c) {
 }
 
 // Tile-shape autotuner. The sandwich and two-sandwich passes of lines of 256 to 2048 points are
-// built in NSHAPES shapes (PassShape: the default, half and twice the lines per CTA). Per (device,
+// built in up to NSHAPES shapes (PassShape: the default, half and twice the lines per CTA, and seven
+// lines per CTA at L = 1024). Per (device,
 // precision, points, line length, stride, pass kind) the first launch outside a stream capture times
 // the pass itself with each shape (its reductions left out) on a zeroed scratch state: one warm-up
 // and three launches each, untimed by the launch counters. A variant replaces the default only when
@@ -885,9 +896,10 @@ static int shape_choice(qnd_ctx* c, const PassSpec& ps, int L, int log2S, int km
     c->shape_buf.reset();  // after the event wait above: no launch reads it any more
     if (const char* logf = std::getenv("QND_TUNE_LOG")) {
         if (FILE* f = std::fopen(logf, "a")) {
-            std::fprintf(f, "%s\tn=%lld\tL=%d\tlog2S=%d\t%s\tms=%.4f,%.4f,%.4f\tchoice=%d\n", c->fp64 ? "fp64" : "fp32",
-                         (long long)c->n, L, log2S, mode == PM_DOUBLE ? "double" : "sandwich", ms[0], ms[1], ms[2],
-                         choice);
+            std::fprintf(f, "%s\tn=%lld\tL=%d\tlog2S=%d\t%s\tms=", c->fp64 ? "fp64" : "fp32", (long long)c->n, L,
+                         log2S, mode == PM_DOUBLE ? "double" : "sandwich");
+            for (int v = 0; v < NSHAPES; ++v) std::fprintf(f, v ? ",%.4f" : "%.4f", ms[v]);
+            std::fprintf(f, "\tchoice=%d\n", choice);
             std::fclose(f);
         }
     }
@@ -922,6 +934,8 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     const int var = c->recorder ? 0 : (ps.force_shape >= 0 ? ps.force_shape : shape_choice(c, ps, L, log2S, kmode));
     const PassKernelInfo info = lookup_pass(c->fp64, L, strided, kmode, var);
     if (!info.fn) QND_FAIL(QND_EINVAL, "internal: no pass kernel for L=%d, mode %d, shape %d", L, kmode, var);
+    if (var != 0 && info.E != lookup_pass(c->fp64, L, strided, kmode, 0).E)
+        QND_FAIL(QND_EINVAL, "internal: shape %d of L=%d has its own FFT plan", var, L);  // every shape shares the plan
     const long long nlines = c->n / L;
     const long long ngroups = (nlines + info.G - 1) / info.G;
     if (c->recorder) {
@@ -945,6 +959,7 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         auto record = [&](auto& a) {
             using A = std::remove_reference_t<decltype(a)>;
             a.red = red;
+            set_red_axes(c, a.red);
             a.log2S = log2S;
             a.nlines = nlines;
             a.use_tma = 0;
@@ -1014,6 +1029,7 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         PassArgs<double> a;
         fill_args<double>(c, ps, a);
         a.red = red;
+        set_red_axes(c, a.red);
         a.tw = static_cast<const double2*>(tw);
         a.log2S = log2S;
         a.nlines = nlines;
@@ -1024,6 +1040,7 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         PassArgs<float> a;
         fill_args<float>(c, ps, a);
         a.red = red;
+        set_red_axes(c, a.red);
         a.tw = static_cast<const float2*>(tw);
         a.log2S = log2S;
         a.nlines = nlines;

@@ -71,6 +71,10 @@ struct RedDesc {
     int kind[MAX_RED];
     int wkind[MAX_RED];
     int waxis[MAX_RED];
+    // WK_AXIS: the weight axis' log2 stride and index mask (set by the host from waxis, so that the
+    // pass kernels index no parameter array by a run-time value)
+    int wshift[MAX_RED];
+    long long wmask[MAX_RED];
     const double* wtab[MAX_RED];
     double scale[MAX_RED];
     double* partials;            // [gridDim.x][MAX_RED] scratch
@@ -131,9 +135,11 @@ template <typename R> struct PassArgs {
 //
 // Shape variants VAR (the tile-shape autotuner picks one per geometry by timing, shape_choice in
 // qnd_engine.cu): 0 the default, 1 half the lines per CTA (smaller CTAs, more of them per SM),
-// 2 twice the lines per CTA (256-thread CTAs). Variants exist for the two-sandwich and sandwich
-// passes of lines of 256 to 2048 points; VALID says whether a variant differs from the default.
-constexpr int NSHAPES = 3;
+// 2 twice the lines per CTA (256-thread CTAs), 3 seven lines per CTA at L = 1024 (448 threads, one
+// CTA per SM: a 1024-line pass then runs as 147 CTAs, 7 lines on every SM, where 2-line CTAs leave
+// some SMs 8 lines and others 6). Variants exist for the two-sandwich and sandwich passes of lines
+// of 256 to 2048 points; VALID says whether a variant differs from the default.
+constexpr int NSHAPES = 4;
 template <typename R, int L, int VAR = 0> struct PassShape {
     // FP64, L >= 1024: 32 values per thread (two radix-32 stages at L = 1024), one CTA per line, a
     // single warp per line at L = 1024 (warp-synchronous exchanges). Otherwise 16 values per thread
@@ -142,8 +148,10 @@ template <typename R, int L, int VAR = 0> struct PassShape {
     static constexpr int E = L <= 16 ? L : (WIDE ? 32 : 16);
     static constexpr int T = L / E;
     static constexpr int G0 = WIDE ? 1 : (T >= 128 ? 1 : 128 / T);
-    static constexpr int G = VAR == 1 ? (G0 > 1 ? G0 / 2 : 1) : (VAR == 2 ? 2 * G0 : G0);
-    static constexpr bool VALID = VAR == 0 || (L >= 256 && L <= 2048 && (VAR == 1 ? G0 > 1 : (T > 32 ? G <= 15 : true)));
+    static constexpr int G = VAR == 1 ? (G0 > 1 ? G0 / 2 : 1) : (VAR == 2 ? 2 * G0 : (VAR == 3 ? 7 : G0));
+    static constexpr bool VALID =
+        VAR == 0 || (VAR == 3 ? (L == 1024 && T == 64)
+                              : (L >= 256 && L <= 2048 && (VAR == 1 ? G0 > 1 : (T > 32 ? G <= 15 : true))));
     static constexpr int NT = T * G;
     static constexpr bool EXCHANGE = FFTPlan<L, E>::NSTAGE > 1;
     static constexpr int SLOTS = sizeof(R) == 8 ? 8 : 16;  // element slots per bank cycle (16 B / 8 B values)
@@ -302,9 +310,8 @@ __device__ __forceinline__ void accumulate_line(const RedDesc& rd, double* acc, 
             if (wk == WK_GRID) {
                 row = wt + lbase + tid;
             } else if (wk == WK_AXIS) {
-                const int ax = rd.waxis[k];
-                if (ax == axis) row = wt + tid;
-                else wl = __ldg(wt + ((base >> shift[ax]) & nmask[ax]));
+                if (rd.waxis[k] == axis) row = wt + tid;
+                else wl = __ldg(wt + ((base >> rd.wshift[k]) & rd.wmask[k]));
             }
             if (row) {
 #pragma unroll
@@ -327,7 +334,7 @@ __device__ __forceinline__ void accumulate_line(const RedDesc& rd, double* acc, 
                 const long long flat = base + ((long long)m << log2S);
                 const cplx_t<R> p = partner[flat];
                 double val = double(p.x) * double(v[u].x) + double(p.y) * double(v[u].y);
-                if (wk == WK_AXIS) val *= __ldg(wt + ((flat >> shift[rd.waxis[k]]) & nmask[rd.waxis[k]]));
+                if (wk == WK_AXIS) val *= __ldg(wt + ((flat >> rd.wshift[k]) & rd.wmask[k]));
                 else if (wk == WK_GRID) val *= __ldg(wt + lbase + m);
                 sum += val;
             }
@@ -409,10 +416,16 @@ __device__ __forceinline__ void apply_factors(cplx_t<R>* v, int tid, long long b
     V lf = fone<V>();
     R lr = R(1);
     bool use_lf = false, use_lr = false;
-    const V* __restrict__ pc = axc ? axc[axis] : nullptr;
-    const R* __restrict__ pr = axr ? axr[axis] : nullptr;
+    // the pass axis' tables picked by a compile-time index (no run-time indexing of the argument
+    // arrays, which would copy them to local memory)
+    const V* __restrict__ pc = nullptr;
+    const R* __restrict__ pr = nullptr;
 #pragma unroll
     for (int k = 0; k < MAX_DIM; ++k) {
+        if (k == axis) {
+            if (axc) pc = axc[k];
+            if (axr) pr = axr[k];
+        }
         if (k >= dim || k == axis) continue;
         const long long ik = (base >> shift[k]) & nmask[k];
         if (axc && axc[k]) { lf = fcompose(lf, axc[k][ik]); use_lf = true; }

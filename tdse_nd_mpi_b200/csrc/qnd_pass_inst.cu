@@ -30,6 +30,7 @@ template <typename R, int L, int VAR> static PassKernelInfo variant_info(bool st
 template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int mode, int var) {
     if (var == 1) return variant_info<R, L, 1>(strided, mode);
     if (var == 2) return variant_info<R, L, 2>(strided, mode);
+    if (var == 3) return variant_info<R, L, 3>(strided, mode);
     using SH = PassShape<R, L>;
     const void* fn = nullptr;
 #define QND_PICK(M) \
