@@ -422,11 +422,12 @@ __device__ __forceinline__ void apply_factors(cplx_t<R>* v, int tid, long long b
     const R* __restrict__ pr = nullptr;
 #pragma unroll
     for (int k = 0; k < MAX_DIM; ++k) {
+        if (k >= dim) break;  // the grid's axes only (a 2-D pass runs two turns of the six)
         if (k == axis) {
             if (axc) pc = axc[k];
             if (axr) pr = axr[k];
+            continue;
         }
-        if (k >= dim || k == axis) continue;
         const long long ik = (base >> shift[k]) & nmask[k];
         if (axc && axc[k]) { lf = fcompose(lf, axc[k][ik]); use_lf = true; }
         if (axr && axr[k]) { lr *= axr[k][ik]; use_lr = true; }
