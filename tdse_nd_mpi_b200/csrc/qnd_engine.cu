@@ -661,7 +661,11 @@ static bool strided_tma_map(qnd_ctx* c, const void* psi, int L, int log2S, int G
     if (std::getenv("QND_NO_TMA")) return false;
     const int64_t S = int64_t(1) << log2S;
     const size_t ce = c->elem();
-    if (reinterpret_cast<uintptr_t>(psi) % 16 || S < G || (size_t(G) * ce) % 16 || (c->n / L) % G) return false;
+    // boxes of G neighbouring lines: every group inside one slab of S lines (G divides S, or the pass
+    // has a single slab; a last group with fewer lines loads past the last line, which reads the fill
+    // value, and stores its lines without boxes)
+    const int64_t slabs = c->n / (S * L);
+    if (reinterpret_cast<uintptr_t>(psi) % 16 || S < G || (size_t(G) * ce) % 16 || (S % G && slabs != 1)) return false;
     const auto key = std::make_tuple(psi, L * 64 + G, log2S);  // G <= 32 lines per box
     auto it = c->tmaps.find(key);
     if (it != c->tmaps.end()) {

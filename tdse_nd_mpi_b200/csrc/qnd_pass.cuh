@@ -551,7 +551,8 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
     if constexpr (STRIDED) {
         if (a.use_tma) {
             // the CTA's G lines as L/BOXL boxes {G lines, BOXL rows} in [row][line] order, loaded by TMA
-            // (the host enables this only when every group is full and the boxes meet the 16-byte rules)
+            // (the host enables this only when every group lies inside one slab of lines and the boxes
+            // meet the 16-byte rules; a partial last group reads the fill value past the last line)
             __shared__ __align__(8) uint64_t tma_bar;
             __shared__ int tma_gave_up;
             constexpr int BOXL = L < 256 ? L : 256;
@@ -736,7 +737,15 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
 
     if (store_out) {
         if constexpr (STRIDED) {
-            if (a.use_tma) {
+            if (a.use_tma && g * G + G > nlines) {
+                // the last group of a pass whose line count G does not divide: its boxes were loaded
+                // with the missing lines filled in, and its lines go back by plain stores (a box store
+                // would reach past the tensor)
+                if (active) {
+#pragma unroll
+                    for (int u = 0; u < E; ++u) a.psi[base + ((long long)(tid + u * T) << log2S)] = v[u];
+                }
+            } else if (a.use_tma) {
                 // the G lines back in [row][line] order, then one thread stores the boxes
                 constexpr int BOXL = L < 256 ? L : 256;
                 __syncthreads();  // every line is done with its exchange buffer
