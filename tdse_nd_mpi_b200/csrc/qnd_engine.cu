@@ -96,10 +96,11 @@ struct DevBuf {
     template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
-static PassKernelInfo lookup_pass(bool fp64, int L, bool strided, int mode, int var = 0) {
+static PassKernelInfo lookup_pass(bool fp64, int L, bool strided, int mode, int var = 0, bool tma = false) {
 #define QND_CASE(LL)                                                                                              \
     case LL:                                                                                                      \
-        return fp64 ? pass_kernel_info<double, LL>(strided, mode, var) : pass_kernel_info<float, LL>(strided, mode, var);
+        return fp64 ? pass_kernel_info<double, LL>(strided, mode, var, tma)                                       \
+                    : pass_kernel_info<float, LL>(strided, mode, var, tma);
     switch (L) {
         QND_CASE(2) QND_CASE(4) QND_CASE(8) QND_CASE(16) QND_CASE(32) QND_CASE(64) QND_CASE(128) QND_CASE(256)
         QND_CASE(512) QND_CASE(1024) QND_CASE(2048) QND_CASE(4096)
@@ -986,16 +987,21 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         return;
     }
     const int staging = !strided ? 0 : ps.force_staging >= 0 ? ps.force_staging : staging_choice(c, ps, L, log2S);
+    // TMA box staging: the tensor map first, then the instantiation compiled for it
+    CUtensorMap tmap{};
+    const bool use_tma = strided && staging && strided_tma_map(c, ps.psi, L, log2S, info.G, &tmap);
+    const PassKernelInfo kinfo = use_tma ? lookup_pass(c->fp64, L, strided, kmode, var, true) : info;
+    if (!kinfo.fn) QND_FAIL(QND_EINVAL, "internal: no TMA pass kernel for L=%d, mode %d, shape %d", L, kmode, var);
     // per (kernel, device), shared by the contexts of every host thread
     static std::map<std::pair<const void*, int>, LaunchCfg> configured;
     static std::mutex configured_mu;
     {
         std::lock_guard<std::mutex> lk(configured_mu);
-        auto cfg_key = std::make_pair(info.fn, c->device);
+        auto cfg_key = std::make_pair(kinfo.fn, c->device);
         if (configured.find(cfg_key) == configured.end()) {
-            QND_CK(cudaFuncSetAttribute(info.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(info.smem)));
+            QND_CK(cudaFuncSetAttribute(kinfo.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kinfo.smem)));
             LaunchCfg cfg;
-            QND_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cfg.blocks_per_sm, info.fn, info.nt, info.smem));
+            QND_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cfg.blocks_per_sm, kinfo.fn, kinfo.nt, kinfo.smem));
             if (cfg.blocks_per_sm < 1) QND_FAIL(QND_ECUDA, "pass kernel for L=%d does not fit on an SM", L);
             configured.emplace(cfg_key, cfg);
         }
@@ -1021,8 +1027,8 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     }
     cudaLaunchConfig_t lc{};
     lc.gridDim = dim3(unsigned(blocks));
-    lc.blockDim = dim3(unsigned(info.nt));
-    lc.dynamicSmemBytes = info.smem;
+    lc.blockDim = dim3(unsigned(kinfo.nt));
+    lc.dynamicSmemBytes = kinfo.smem;
     lc.stream = c->stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1037,9 +1043,10 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         a.tw = static_cast<const double2*>(tw);
         a.log2S = log2S;
         a.nlines = nlines;
-        if (strided && staging) a.use_tma = strided_tma_map(c, ps.psi, L, log2S, info.G, &a.tmap) ? 1 : 0;
+        a.use_tma = use_tma ? 1 : 0;
+        if (use_tma) a.tmap = tmap;
         void* args[] = {&a};
-        QND_CK(cudaLaunchKernelExC(&lc, info.fn, args));
+        QND_CK(cudaLaunchKernelExC(&lc, kinfo.fn, args));
     } else {
         PassArgs<float> a;
         fill_args<float>(c, ps, a);
@@ -1048,9 +1055,10 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         a.tw = static_cast<const float2*>(tw);
         a.log2S = log2S;
         a.nlines = nlines;
-        if (strided && staging) a.use_tma = strided_tma_map(c, ps.psi, L, log2S, info.G, &a.tmap) ? 1 : 0;
+        a.use_tma = use_tma ? 1 : 0;
+        if (use_tma) a.tmap = tmap;
         void* args[] = {&a};
-        QND_CK(cudaLaunchKernelExC(&lc, info.fn, args));
+        QND_CK(cudaLaunchKernelExC(&lc, kinfo.fn, args));
     }
     c->kernels_launched++;
     if (c->profiling) {

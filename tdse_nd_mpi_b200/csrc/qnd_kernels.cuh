@@ -16,7 +16,8 @@ struct PassKernelInfo {
 
 // Defined once per line length in qnd_pass_inst.cu (compiled with -DQND_L=...). var: the shape
 // variant (PassShape); fn is null where a variant does not exist.
-template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int mode, int var = 0);
+// tma: the strided instantiation that stages its lines by TMA boxes (the host has a tensor map for it)
+template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int mode, int var = 0, bool tma = false);
 
 // Host-side copy of the FFTPlan stage structure for a runtime line length.
 struct HostPlan {

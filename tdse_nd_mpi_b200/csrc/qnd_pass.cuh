@@ -495,9 +495,13 @@ __device__ __forceinline__ void apply_factors(cplx_t<R>* v, int tid, long long b
 // memory smem_raw. `wait` runs after the prologue (twiddles to shared memory, read-only tables to
 // L2), before the state is touched: the wait for the previous pass (programmatic dependent launch
 // in qnd_pass_kernel, the pass's dependency counter in the persistent sweep kernel).
-template <typename R, int L, bool STRIDED, int KMODE, int VAR = 0, typename Wait>
+// SK: 0 a contiguous axis, 1 a strided axis staged by per-thread cp.async copies, 2 a strided axis
+// staged by TMA boxes (separate instantiations: each staging gets its own register allocation).
+template <typename R, int L, int SK, int KMODE, int VAR = 0, typename Wait>
 __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, unsigned ngroups,
                                            unsigned char* smem_raw, Wait wait) {
+    constexpr bool STRIDED = SK != 0;
+    constexpr bool TMA = SK == 2;
     constexpr int MODE = pass_base_mode(KMODE);
     constexpr bool HAS_RED = pass_mode_reduces(KMODE);
     using V = cplx_t<R>;
@@ -549,7 +553,7 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
 
     V v[E];
     if constexpr (STRIDED) {
-        if (a.use_tma) {
+        if constexpr (TMA) {
             // the CTA's G lines as L/BOXL boxes {G lines, BOXL rows} in [row][line] order, loaded by TMA
             // (the host enables this only when every group lies inside one slab of lines and the boxes
             // meet the 16-byte rules; a partial last group reads the fill value past the last line)
@@ -620,7 +624,7 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
                                    nullptr, a.axis, a.dim, a.shift, a.nmask, a.pro_scale_dev, key0 ^ 0x51ed270bu);
     }
     if constexpr (STRIDED) {
-        if (!a.use_tma) lsync();  // staged inputs read before the exchanges reuse the buffer
+        if constexpr (!TMA) lsync();  // staged inputs read before the exchanges reuse the buffer
     }
 
     double acc[MAX_RED];
@@ -737,7 +741,7 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
 
     if (store_out) {
         if constexpr (STRIDED) {
-            if (a.use_tma && g * G + G > nlines) {
+            if (TMA && g * G + G > nlines) {
                 // the last group of a pass whose line count G does not divide: its boxes were loaded
                 // with the missing lines filled in, and its lines go back by plain stores (a box store
                 // would reach past the tensor)
@@ -745,7 +749,7 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
 #pragma unroll
                     for (int u = 0; u < E; ++u) a.psi[base + ((long long)(tid + u * T) << log2S)] = v[u];
                 }
-            } else if (a.use_tma) {
+            } else if constexpr (TMA) {
                 // the G lines back in [row][line] order, then one thread stores the boxes
                 constexpr int BOXL = L < 256 ? L : 256;
                 __syncthreads();  // every line is done with its exchange buffer
@@ -785,11 +789,11 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
         if (MODE == PM_SPECRED || (a.red.n && !a.red_at_mid)) finish_red<NT>(a.red, acc, unsigned(g), ngroups);
 }
 
-template <typename R, int L, bool STRIDED, int KMODE, int VAR = 0>
+template <typename R, int L, int SK, int KMODE, int VAR = 0>
 __global__ void __launch_bounds__(PassShape<R, L, VAR>::NT, PassShape<R, L, VAR>::MINB)
     qnd_pass_kernel(const __grid_constant__ PassArgs<R> a) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    pass_group<R, L, STRIDED, KMODE, VAR>(a, blockIdx.x, gridDim.x, smem_raw, [] {
+    pass_group<R, L, SK, KMODE, VAR>(a, blockIdx.x, gridDim.x, smem_raw, [] {
         pdl_wait();
         pdl_launch_dependents();
     });

@@ -41,7 +41,7 @@ __device__ __forceinline__ bool sweep_wait(const unsigned* done, unsigned need, 
 
 template <typename R, int L, bool S, int KM>
 __device__ __noinline__ void sweep_run(const SweepSlot& sl, long long g, unsigned char* smem) {
-    pass_group<R, L, S, KM, 0>(*static_cast<const PassArgs<R>*>(sl.args), g, sl.ngroups, smem, [] {});
+    pass_group<R, L, S ? 1 : 0, KM, 0>(*static_cast<const PassArgs<R>*>(sl.args), g, sl.ngroups, smem, [] {});
 }
 
 template <typename R, int L, bool S>
