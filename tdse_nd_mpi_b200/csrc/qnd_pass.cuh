@@ -679,8 +679,13 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
                                                  a.nmask);
                 }
                 // finish those reductions here, so that no accumulator stays live through the second sandwich
-                if constexpr (HAS_RED)
+                if constexpr (HAS_RED) {
                     if (a.red_at_mid && a.red.n) finish_red<NT>(a.red, acc, unsigned(g), ngroups);
+                    // zero again whichever branch ran (the end reductions start from zero either way):
+                    // the compiler then holds no accumulator across the second sandwich
+#pragma unroll
+                    for (int k = 0; k < MAX_RED; ++k) acc[k] = 0.0;
+                }
             }
         }
         if (active) {
