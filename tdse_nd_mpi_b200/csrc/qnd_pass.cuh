@@ -167,7 +167,11 @@ template <typename R, int L, int VAR = 0> struct PassShape {
     static constexpr bool TW_SMEM = G > 1 && size_t(TWN_RAW) * sizeof(cplx_t<R>) <= 16 * 1024;
     // the line buffers start on a 128-byte boundary (TMA box destinations)
     static constexpr int TWN = TW_SMEM ? ((TWN_RAW * int(sizeof(cplx_t<R>)) + 127) / 128 * 128) / int(sizeof(cplx_t<R>)) : 0;
-    static constexpr size_t SMEM = sizeof(cplx_t<R>) * (size_t(TWN) + size_t(G) * LS);
+    // the 7-line shape (one CTA per SM, shared memory to spare) keeps the spectral rows of both
+    // sandwiches in shared memory: read by 7 lines each, once per CTA from L2
+    static constexpr bool SPEC_SMEM = VAR == 3;
+    static constexpr int SPECN = SPEC_SMEM ? 2 * L : 0;
+    static constexpr size_t SMEM = sizeof(cplx_t<R>) * (size_t(TWN) + size_t(G) * LS + size_t(SPECN));
     // 128-thread CTAs: <= 128 registers (4 CTAs per SM) when shared memory allows; one-line CTAs
     // of L >= 1024 keep their registers (the SM holds as many lines as its register file allows)
     static constexpr int MINB_DEFAULT =
@@ -510,6 +514,7 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
     constexpr bool TWS = SH::TW_SMEM;
     V* tw_s = reinterpret_cast<V*>(smem_raw);   // [TWN] stage twiddles (when they fit)
     V* lines = tw_s + SH::TWN;                   // [G][LS]
+    V* spec_s = lines + G * LS;                  // [2][L] spectral rows (SPEC_SMEM)
 
     const int t = threadIdx.x;
     const int w = t / T;  // line within the CTA (the threads of a line are consecutive)
@@ -532,6 +537,15 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
     if constexpr (TWS) {
         for (int i = t; i < SH::TW_ENTRIES; i += NT) tw_s[i] = a.tw[i];
         tw = tw_s;
+    }
+    // spectral rows to shared memory (read-only tables: before the wait for the previous pass);
+    // visible after the CTA barrier that precedes the first transform
+    const bool spec_row = a.spec && !a.spec_full;
+    if constexpr (SH::SPEC_SMEM && (MODE == PM_DOUBLE || MODE == PM_SANDWICH)) {
+        if (spec_row)
+            for (int i = t; i < L; i += NT) spec_s[i] = __ldg(a.spec + i);
+        if (MODE == PM_DOUBLE && a.spec2)
+            for (int i = t; i < L; i += NT) spec_s[L + i] = __ldg(a.spec2 + i);
     }
 
     if constexpr (MODE == PM_DOUBLE || MODE == PM_SANDWICH) {
@@ -664,9 +678,17 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
             const V* __restrict__ sp = half ? a.spec2 : (a.spec ? a.spec + (a.spec_full ? lbase : 0ll) : nullptr);
             if (sp) {
                 const uint32_t kh = key0 + uint32_t(half * L);
+                if (SH::SPEC_SMEM && (half || spec_row)) {
+                    const V* sps = spec_s + (half ? L : 0);
 #pragma unroll
-                for (int u = 0; u < E; ++u)
-                    v[u] = fmul_spec<L>(v[u], __ldg(sp + tid + u * T), kh + uint32_t(tid + u * T), u == 0 || u == E - 1);
+                    for (int u = 0; u < E; ++u)
+                        v[u] = fmul_spec<L>(v[u], sps[tid + u * T], kh + uint32_t(tid + u * T), u == 0 || u == E - 1);
+                } else {
+#pragma unroll
+                    for (int u = 0; u < E; ++u)
+                        v[u] = fmul_spec<L>(v[u], __ldg(sp + tid + u * T), kh + uint32_t(tid + u * T),
+                                            u == 0 || u == E - 1);
+                }
             }
             fft_line_stages<L, E, +1, 0, TWS>(v, tid, line, tw, lsync);
             if (half == 0) {
@@ -704,9 +726,16 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
         // SANDWICH / APPLY: spectral multiply, inverse transform
         if (a.spec) {
             const V* __restrict__ sp = a.spec + (a.spec_full ? lbase : 0ll);
+            if (SH::SPEC_SMEM && MODE == PM_SANDWICH && spec_row) {
 #pragma unroll
-            for (int u = 0; u < E; ++u)
-                v[u] = fmul_spec<L>(v[u], __ldg(sp + tid + u * T), key0 + uint32_t(tid + u * T), u == 0 || u == E - 1);
+                for (int u = 0; u < E; ++u)
+                    v[u] = fmul_spec<L>(v[u], spec_s[tid + u * T], key0 + uint32_t(tid + u * T), u == 0 || u == E - 1);
+            } else {
+#pragma unroll
+                for (int u = 0; u < E; ++u)
+                    v[u] = fmul_spec<L>(v[u], __ldg(sp + tid + u * T), key0 + uint32_t(tid + u * T),
+                                        u == 0 || u == E - 1);
+            }
         }
         fft_line_stages<L, E, +1, 0, TWS>(v, tid, line, tw, lsync);
         if (active) {
