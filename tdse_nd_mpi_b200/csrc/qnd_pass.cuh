@@ -384,19 +384,30 @@ __device__ __forceinline__ void finish_red(const RedDesc& rd, double* acc, unsig
     __syncthreads();
     if (!is_last) return;
     __threadfence();
-    for (int k = 0; k < rd.n; ++k) {
-        double s = 0.0;
-        for (unsigned b = t; b < nblk; b += NT) s += __ldcg(rd.partials + (long long)b * MAX_RED + k);
-        s = warp_sum(s);
-        if (lane == 0) red_s[wid][k] = s;
-        __syncthreads();
-        if (t == 0) {
-            double tot = 0.0;
-            for (int w = 0; w < NW; ++w) tot += red_s[w][k];
-            tot *= rd.scale[k];
-            rd.out[k] = rd.accumulate ? rd.out[k] + tot : tot;
-        }
-        __syncthreads();
+    // every accumulator in one sweep over the partials (one round of L2 loads, one barrier): the
+    // last CTA's tail is the critical path of the pass. Per accumulator the order of the sums is
+    // the same as one accumulator at a time (thread-strided partials, warp sum, warps in order).
+    double s[MAX_RED];
+#pragma unroll
+    for (int k = 0; k < MAX_RED; ++k) s[k] = 0.0;
+    for (unsigned b = t; b < nblk; b += NT) {
+        const double* pb = rd.partials + (long long)b * MAX_RED;
+#pragma unroll
+        for (int k = 0; k < MAX_RED; ++k)
+            if (k < rd.n) s[k] += __ldcg(pb + k);
+    }
+#pragma unroll
+    for (int k = 0; k < MAX_RED; ++k) {
+        if (k >= rd.n) break;
+        const double ws = warp_sum(s[k]);
+        if (lane == 0) red_s[wid][k] = ws;
+    }
+    __syncthreads();
+    if (t < rd.n) {
+        double tot = 0.0;
+        for (int w = 0; w < NW; ++w) tot += red_s[w][t];
+        tot *= rd.scale[t];
+        rd.out[t] = rd.accumulate ? rd.out[t] + tot : tot;
     }
     if (t == 0) *rd.counter = 0u;
 }
