@@ -934,7 +934,7 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
     // registers for the transform
     int kmode = ps.mode;
     if (ps.red.n && ps.mode == PM_SANDWICH) kmode = PM_SANDWICH_RED;
-    if (ps.red.n && ps.mode == PM_DOUBLE) kmode = PM_DOUBLE_RED;
+    if (ps.red.n && ps.mode == PM_DOUBLE) kmode = ps.red_at_mid ? PM_DOUBLE_RED : PM_DOUBLE_RED_END;
     // the shape variant: the default while recording (the sweep kernel holds the default shapes)
     const int var = c->recorder ? 0 : (ps.force_shape >= 0 ? ps.force_shape : shape_choice(c, ps, L, log2S, kmode));
     const PassKernelInfo info = lookup_pass(c->fp64, L, strided, kmode, var);
@@ -947,7 +947,7 @@ static void launch_pass(qnd_ctx* c, const PassSpec& ps) {
         // qnd_run_length_sweep: the arguments this launch would get (per-thread staging: the sweep
         // kernel takes its arguments from device memory), kept for the persistent kernel
         if (!sweep_length_ok(L) || ps.vL || (kmode != PM_SANDWICH && kmode != PM_SANDWICH_RED && kmode != PM_DOUBLE &&
-                                             kmode != PM_DOUBLE_RED))
+                                             kmode != PM_DOUBLE_RED && kmode != PM_DOUBLE_RED_END))
             QND_FAIL(QND_EUNSUPPORTED, "qnd_run_length_sweep: a pass of line length %d, mode %d is outside the "
                                        "sweep kernel (axis lengths 128 to 1024)", L, kmode);
         RecordedPass rp;

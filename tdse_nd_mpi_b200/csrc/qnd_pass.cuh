@@ -49,16 +49,17 @@ enum : int {
     PM_DOUBLE = 5,
     PM_ROUNDTRIP = 6,
     PM_SANDWICH_RED = 7,  // PM_SANDWICH / PM_DOUBLE with fused reductions: separate instantiations, so that
-    PM_DOUBLE_RED = 8,    // the passes without reductions (most of a chain) keep their registers for the FFT
-    PM_NMODES = 9
+    PM_DOUBLE_RED = 8,    // the passes without reductions (most of a chain) keep their registers for the FFT;
+    PM_DOUBLE_RED_END = 9,  // PM_DOUBLE_RED reduces between its sandwiches (a step boundary), _END after both
+    PM_NMODES = 10
 };
 // The transform structure of a mode (the reducing variants share their base mode's) and whether the
 // mode can carry reductions at all.
 __host__ __device__ constexpr int pass_base_mode(int m) {
-    return m == PM_SANDWICH_RED ? PM_SANDWICH : (m == PM_DOUBLE_RED ? PM_DOUBLE : m);
+    return m == PM_SANDWICH_RED ? PM_SANDWICH : ((m == PM_DOUBLE_RED || m == PM_DOUBLE_RED_END) ? PM_DOUBLE : m);
 }
 __host__ __device__ constexpr bool pass_mode_reduces(int m) {
-    return m == PM_SANDWICH_RED || m == PM_DOUBLE_RED || m == PM_SPECRED || m == PM_APPLY;
+    return m == PM_SANDWICH_RED || m == PM_DOUBLE_RED || m == PM_DOUBLE_RED_END || m == PM_SPECRED || m == PM_APPLY;
 }
 // |v|^2 w, Re(conj(partner) v) w, or (element-wise grid reductions only) Im(conj(partner) v) w and
 // the count of elements with a non-finite part
@@ -519,6 +520,8 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
     constexpr bool TMA = SK == 2;
     constexpr int MODE = pass_base_mode(KMODE);
     constexpr bool HAS_RED = pass_mode_reduces(KMODE);
+    // two-sandwich passes: reductions between the sandwiches, or after both (compile-time)
+    constexpr bool RED_MID = KMODE == PM_DOUBLE_RED, RED_END = KMODE == PM_DOUBLE_RED_END;
     using V = cplx_t<R>;
     using SH = PassShape<R, L, VAR>;
     constexpr int E = SH::E, T = SH::T, G = SH::G, NT = SH::NT, LS = SH::LS;
@@ -707,13 +710,13 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
                     apply_factors<R, E, T>(v, tid, base, lbase, a.mid_real, a.mid_cplx, a.mid_ax_cplx, a.mid_ax_real,
                                            a.axis, a.dim, a.shift, a.nmask, nullptr, key0 ^ 0x2545f491u);
                     // a step boundary inside the pass: observables of the state between the two steps
-                    if (HAS_RED && a.red_at_mid && a.red.n)
+                    if (RED_MID && a.red.n)
                         accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift,
                                                  a.nmask);
                 }
                 // finish those reductions here, so that no accumulator stays live through the second sandwich
                 if constexpr (HAS_RED) {
-                    if (a.red_at_mid && a.red.n) finish_red<NT>(a.red, acc, unsigned(g), ngroups);
+                    if (RED_MID && a.red.n) finish_red<NT>(a.red, acc, unsigned(g), ngroups);
                     // zero again whichever branch ran (the end reductions start from zero either way):
                     // the compiler then holds no accumulator across the second sandwich
 #pragma unroll
@@ -729,7 +732,7 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
                 apply_factors<R, E, T>(v, tid, base, lbase, nullptr, nullptr, nullptr, a.ax_real, a.axis, a.dim,
                                        a.shift, a.nmask, nullptr, key0 ^ 0x68e31da4u);
             // the end of a chain of 1-D sandwich pairs: reductions of the final state
-            if (HAS_RED && a.red.n && !a.red_at_mid)
+            if (RED_END && a.red.n)
                 accumulate_line<R, E, T>(a.red, acc, v, a.partner, base, log2S, lbase, tid, a.axis, a.shift, a.nmask);
         }
         store_out = true;
@@ -831,7 +834,8 @@ __device__ __forceinline__ void pass_group(const PassArgs<R>& a, long long g, un
         }
     }
     if constexpr (HAS_RED)
-        if (MODE == PM_SPECRED || (a.red.n && !a.red_at_mid)) finish_red<NT>(a.red, acc, unsigned(g), ngroups);
+        if (MODE == PM_SPECRED || (a.red.n && (MODE == PM_DOUBLE ? RED_END : !a.red_at_mid)))
+            finish_red<NT>(a.red, acc, unsigned(g), ngroups);
 }
 
 template <typename R, int L, int SK, int KMODE, int VAR = 0>

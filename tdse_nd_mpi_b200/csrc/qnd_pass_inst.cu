@@ -24,6 +24,7 @@ template <typename R, int L, int VAR> static PassKernelInfo variant_info(int sk,
         case PM_DOUBLE: fn = QND_PICKV(PM_DOUBLE); break;
         case PM_SANDWICH_RED: fn = QND_PICKV(PM_SANDWICH_RED); break;
         case PM_DOUBLE_RED: fn = QND_PICKV(PM_DOUBLE_RED); break;
+        case PM_DOUBLE_RED_END: fn = QND_PICKV(PM_DOUBLE_RED_END); break;
         default: fn = nullptr;
         }
 #undef QND_PICKV
@@ -49,6 +50,7 @@ template <typename R, int L> PassKernelInfo pass_kernel_info(bool strided, int m
     case PM_ROUNDTRIP: fn = QND_PICK(PM_ROUNDTRIP); break;
     case PM_SANDWICH_RED: fn = QND_PICK(PM_SANDWICH_RED); break;
     case PM_DOUBLE_RED: fn = QND_PICK(PM_DOUBLE_RED); break;
+    case PM_DOUBLE_RED_END: fn = QND_PICK(PM_DOUBLE_RED_END); break;
     default: fn = nullptr;
     }
 #undef QND_PICK

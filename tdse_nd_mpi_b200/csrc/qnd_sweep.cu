@@ -51,6 +51,7 @@ __device__ __forceinline__ void sweep_dispatch_mode(const SweepSlot& sl, long lo
     case PM_SANDWICH_RED: sweep_run<R, L, S, PM_SANDWICH_RED>(sl, g, smem); break;
     case PM_DOUBLE: sweep_run<R, L, S, PM_DOUBLE>(sl, g, smem); break;
     case PM_DOUBLE_RED: sweep_run<R, L, S, PM_DOUBLE_RED>(sl, g, smem); break;
+    case PM_DOUBLE_RED_END: sweep_run<R, L, S, PM_DOUBLE_RED_END>(sl, g, smem); break;
     default: break;  // the host records only these modes
     }
 }
