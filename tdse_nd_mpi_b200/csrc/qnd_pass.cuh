@@ -119,8 +119,8 @@ template <typename R> struct PassArgs {
     const double* apply_vtab;
     RedDesc red;
     // strided passes: the state as a 3-D tensor {contiguous sub-index, pass axis, outer} for TMA box
-    // loads of a CTA's G lines (use_tma = 0: per-thread cp.async staging); err: set when a wait for
-    // those loads runs out
+    // loads of a CTA's G lines, read by the SK = 2 instantiations (use_tma records the host's choice);
+    // err: set when a wait for those loads runs out
     int use_tma;
     int* err;
     int tma_wait_tries;          // tries of the bounded wait for those loads before the CTA gives up
@@ -129,10 +129,11 @@ template <typename R> struct PassArgs {
 };
 
 // Threads-per-line, values-per-thread and lines-per-CTA for a line length.
-//   E values per thread in registers: 32 for L >= 1024 (two radix-32 stages, one warp per line
-//   at L = 1024), else 16. T = L/E threads per line; a CTA of NT = T*G threads owns G lines.
-//   Lines along a strided axis are staged through shared memory with cp.async so that the
-//   global accesses run over G neighbouring lines; the stage buffer is then the exchange space.
+//   E = 16 values per thread in registers (L itself up to 16 points; 32 values per thread, one
+//   warp per 1024-point line, measured slower: WIDE). T = L/E threads per line; a CTA of NT = T*G
+//   threads owns G lines. Lines along a strided axis are staged through shared memory, by
+//   per-thread cp.async copies or by TMA boxes (the kernel's SK), so that the global accesses run
+//   over G neighbouring lines; the stage buffer is then the exchange space.
 //
 // Shape variants VAR (the tile-shape autotuner picks one per geometry by timing, shape_choice in
 // qnd_engine.cu): 0 the default, 1 half the lines per CTA (smaller CTAs, more of them per SM),
